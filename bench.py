@@ -1,0 +1,395 @@
+"""Benchmark of the BSSN RHS + RK4 step on B200.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl b200|reference] [--n 128]
+
+A step is one RK4 step (4 fused RHS+KO+stage launches, enforcement fused
+into the last, 1 time-advance launch) of the 128^3-interior (+3 ghosts,
+134^3 array, 462 MB state) q = 1/10 Brill-Lindquist workload on [-8,8]^3,
+dt = 0.25 dx, KO sigma 0.1 (order 6). The metric is Mpoint-updates/s:
+interior points x 4 RHS evaluations per step / time (the reference's unit,
+3D/src/bssn3d/profile_regime.py:230). Inputs stay in HBM between steps and
+are larger than L2 (126 MB).
+
+For N > 1 (under torchrun) every rank evolves its own replica (the path has
+no exchange step at one block per GPU): weak scaling, value = total work of
+all ranks / max-over-ranks time.
+
+``--impl reference`` times the reference's own CPU algebra
+(oracle/_ref/libdendro_ref.so, compiled from the reference's vendored
+Dendro-GR CSE) with the oracle's restated stencils, KO, RK4 and enforcement
+on all host threads, on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "integer-schemes_b200"))
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+METRIC = "BSSN RHS Mpoint-updates/s (RK4 step, fused FP64)"
+UNIT = "Mpoint-updates/s"
+FLOPS_PER_POINT = 6840      # algorithmic FP64 flops per RHS point-update
+KO_FLOPS_PER_POINT = 936    # 24 fields x 3 axes x (7 taps: 7 mul + 6 add)
+STAGE_BYTES = 960           # read Y, U, ACC; write ACC, Y_next (5 x 24 x 8 B)
+LAST_STAGE_BYTES = 768      # read Y, U, ACC; write U_new
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="interior points per axis")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_step_sample(n_interior: int, planes: int = 8):
+    """A bounded sample of the workload for the CPU reference: `planes`
+    interior x-planes (+3 ghosts each side) of the full-size y-z cross section."""
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.fused_rhs import pack_S
+    grid, U, dt = ID.workload(1, n=n_interior)
+    ng = grid.ng
+    mid = U.shape[1] // 2
+    Us = np.ascontiguousarray(U[:, mid - planes // 2 - ng: mid + planes // 2 + ng])
+    S = pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0), grid.dy, grid.dz)
+    interior = planes * n_interior * n_interior
+    return Us, S, interior
+
+
+def run_cpu_reference(U, S, steps, warmup, threads):
+    """RK4 steps of evolve.py:125-137 with the reference's compiled algebra."""
+    from oracle import oracle as O
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    dt = S[2]
+    g = (S[13], S[14], S[15])
+
+    def rate(Y, tt):
+        S2 = S.copy()
+        S2[6] = tt
+        return O.ref_rhs(Y, S2, nthreads=threads) + O.ko(Y, *g, 0.1, 6)
+
+    def step(U, t):
+        k1 = rate(U, t)
+        k2 = rate(U + 0.5 * dt * k1, t + 0.5 * dt)
+        k3 = rate(U + 0.5 * dt * k2, t + 0.5 * dt)
+        k4 = rate(U + dt * k3, t + dt)
+        return O.enforce(U + (dt / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4))
+
+    t = 0.0
+    for _ in range(warmup):
+        U = step(U, t)
+        t += dt
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        U = step(U, t)
+        times.append(time.perf_counter() - t0)
+        t += dt
+    return times
+
+
+def measure_fp64_peak(torch, dev):
+    """cuBLAS DGEMM throughput on this GPU (TFLOP/s), the FP64 roofline denominator."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    c = torch.empty_like(a)
+    for _ in range(2):
+        torch.matmul(a, b, out=c)
+    torch.cuda.synchronize(dev)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return best
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except ValueError:
+            pass
+    return {"hbm_gbs": 6650.0}, "fallback"
+
+
+# ---------------------------------------------------------------- arms
+def bench_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return
+    threads = cpu_threads()
+    U, S, interior = reference_step_sample(args.n)
+    times = run_cpu_reference(U, S, args.steps, args.warmup, threads)
+    t = sum(times)
+    value = interior * 4 * args.steps / t / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Brill-Lindquist q=1/10, {args.n}^3 interior +3 ghosts on [-8,8]^3, "
+                               f"RK4 step, KO sigma 0.1 order 6",
+                   "sample": f"8 interior x-planes of the {args.n}^2 cross-section (+3 ghosts)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"RK4 steps of an 8x{args.n}x{args.n}-interior slab: reference "
+                                   f"Dendro-GR algebra (oracle/_ref) + restated stencils/KO/enforce"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_b200(args):
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.evolve import BSSNEvolution
+    from bssn3d_b200.state import BSSNState
+    from bssn3d_b200.fused_rhs import Scratch
+
+    grid, U_host, dt = ID.workload(1, n=args.n)
+    interior = grid.interior_points
+    npts = int(np.prod(grid.shape))
+    evo = BSSNEvolution(grid, ko_sigma=0.1, bc="none", ko_order=6)
+    U0 = torch.from_numpy(U_host).to(dev)
+    S0 = evo._S(0.0, dt, dev)
+    graph, U_g, S_g = evo.capture(U0, S0)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        graph.replay()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    finite = bool(torch.isfinite(U_g).all().item())
+
+    # per-launch stage-kernel durations (roofline), on the launching stream
+    stage_ms = []
+    b = evo._buffers(U_g)
+    for s in range(4):
+        Y = U_g if s == 0 else (b["Ya"] if s in (1, 3) else b["Yb"])
+        Yn = {0: b["Ya"], 1: b["Yb"], 2: b["Ya"], 3: b["Yb"]}[s]   # stage 3 timed out of place
+        durs = []
+        for _ in range(3):
+            a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a0.record(stream)
+            evo._stage(s, U_g, Y, b["ACC"], Yn, S_g)
+            a1.record(stream)
+            a1.synchronize()
+            durs.append(a0.elapsed_time(a1))
+        stage_ms.append(statistics.median(durs))
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(U_host).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        for _ in range(2):
+            U_g.copy_(host_in, non_blocking=True)
+            graph.replay()
+            host_out.copy_(U_g, non_blocking=True)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            U_g.copy_(host_in, non_blocking=True)
+            graph.replay()
+            host_out.copy_(U_g, non_blocking=True)
+        f1.record(stream)
+        barrier()
+        ems = f0.elapsed_time(f1)
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = U_host.nbytes
+        e2e = {"value": interior * 4 * args.steps * world / (ems * 1e-3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes,
+               "ms_per_step": ems / args.steps,
+               "path": "BSSNEvolution captured step (C ABI bssn_b200_rk4_stage) with pinned host state in/out"}
+
+    peaks, peak_kind = measured_peaks()
+    fp64_peak = measure_fp64_peak(torch, dev) if rank == 0 else None
+
+    value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
+    mean_stage = statistics.mean(stage_ms[:3])
+    achieved_gbs = npts * STAGE_BYTES / (mean_stage * 1e-3) / 1e9
+    flops = npts * (FLOPS_PER_POINT + KO_FLOPS_PER_POINT)
+    achieved_tf = flops / (mean_stage * 1e-3) / 1e12
+    roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs"),
+                "unit": "GB/s", "frac": achieved_gbs / peaks.get("hbm_gbs"),
+                "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "bssn::fused_kernel<3,MODE_STAGE> (stages 0-2)",
+                "bytes_per_point": STAGE_BYTES, "points_per_launch": npts,
+                "launch_ms": mean_stage}
+    roofline_fp64 = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak,
+                     "unit": "TFLOP/s", "frac": (achieved_tf / fp64_peak) if fp64_peak else None,
+                     "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
+                     "flops_per_point": FLOPS_PER_POINT + KO_FLOPS_PER_POINT}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = cpu_threads()
+            Us, S, inter = reference_step_sample(args.n)
+            times = run_cpu_reference(Us, S, 2, 1, threads)
+            cpu = {"value": inter * 4 * len(times) / sum(times) / 1e6, "unit": UNIT,
+                   "cores": threads, "kind": "reference",
+                   "sample": f"2 RK4 steps of an 8x{args.n}x{args.n}-interior slab: reference "
+                             f"Dendro-GR algebra (oracle/_ref) + restated stencils/KO/enforce"}
+        except (FileNotFoundError, OSError) as exc:
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                   "sample": f"unavailable: {exc}"}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"Brill-Lindquist q=1/10, {args.n}^3 interior +3 ghosts on [-8,8]^3, "
+                               f"RK4 step (4 fused RHS+KO+stage launches), KO sigma 0.1 order 6",
+                   "array": list(grid.shape), "state_bytes": int(U_host.nbytes),
+                   "l2": "inputs larger than L2 (462 MB state)", "parallelism": f"replicas x{world}"},
+        "clocks": clk, "gpu_launches": 5 * args.steps, "finite": finite,
+        "stage_ms": stage_ms, "roofline": roofline, "roofline_fp64": roofline_fp64,
+        "e2e": e2e, "cpu_baseline": cpu,
+    }
+    del graph
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        bench_reference(args)
+    else:
+        bench_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,151 @@
+"""``BSSNEvolution`` — RK4 time integration (3D/src/bssn3d/evolve.py:24-194)
+on the fused B200 stage kernel.
+
+Each RK4 stage is ONE launch of ``bssn_b200_rk4_stage``: derivatives, KO
+dissipation, the BSSN algebra and the stage update (with algebraic
+enforcement after the last stage) in one kernel. A step is four launches
+(+ a ghost sync per stage for periodic boundaries) and ``evolve`` replays the
+step as a captured CUDA graph. Stage times are t, t+dt/2, t+dt/2, t+dt with
+the full dt in the CAHD factor (evolve.py:121-131).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .fused_rhs import Scratch, _stream_handle, as_device_state, device_scalars, scalars
+from .grid import Grid
+from .rhs import BSSNSolver
+from .state import BSSNState, PhysicsParams
+
+
+class BSSNEvolution:
+    def __init__(self, grid: Grid, params: PhysicsParams = None, order: int = 6,
+                 ko_sigma: float = 0.0, bc: str = "periodic", precision: str = "fp64",
+                 scheme: str = "cuda_b200", ko_order: int = 8, integrator: str = "rk4"):
+        self.grid = grid
+        self.params = params or PhysicsParams()
+        self.solver = BSSNSolver(grid, self.params, order, precision=precision,
+                                 scheme=scheme, ko_order=ko_order)
+        self.ng = grid.ng
+        self.ko_sigma = float(ko_sigma)
+        self.ko_order = ko_order
+        if bc not in ("periodic", "none"):
+            raise ValueError(f"unknown bc {bc!r} (periodic or none)")
+        self.bc = bc
+        if integrator != "rk4":
+            raise ValueError(f"integrator {integrator!r} is not provided (rk4 only)")
+        self.integrator = integrator
+        self._bufs = {}
+        self._graph = None
+
+    # ------------------------------------------------------------------
+    def _buffers(self, U: torch.Tensor):
+        key = (tuple(U.shape), U.device)
+        b = self._bufs.get(key)
+        if b is None:
+            b = {name: torch.empty_like(U) for name in ("Ya", "Yb", "ACC")}
+            if self.bc == "periodic":
+                b["Ys"] = torch.empty_like(U)
+            self._bufs = {key: b}
+        return b
+
+    def _S(self, t: float, dt: float, device) -> torch.Tensor:
+        g = self.grid
+        return device_scalars(scalars(self.params, g.dx, g.dy, g.dz, dt, t), device)
+
+    def _stage(self, stage, U, Y, ACC, YNEXT, S):
+        lib = _lib.load()
+        scratch = Scratch.get(U.device)
+        _, Sx, Sy, Sz = U.shape
+        src = Y
+        if self.bc == "periodic":
+            Ys = self._buffers(U)["Ys"]
+            Ys.copy_(Y)
+            _lib.check(lib.bssn_b200_periodic_sync(_stream_handle(U.device), Ys.data_ptr(),
+                                                   Sx, Sy, Sz, self.ng))
+            src = Ys
+        p = self.params
+        rc = lib.bssn_b200_rk4_stage(_stream_handle(U.device), stage, U.data_ptr(), src.data_ptr(),
+                                     ACC.data_ptr(), YNEXT.data_ptr(), S.data_ptr(),
+                                     self.ko_sigma, self.ko_order, p.chi_floor, p.alpha_floor,
+                                     Sx, Sy, Sz, scratch.data_ptr(), scratch.numel() * 8)
+        _lib.check(rc)
+
+    def _advance_time(self, S: torch.Tensor):
+        _lib.check(_lib.load().bssn_b200_advance_time(_stream_handle(S.device), S.data_ptr()))
+
+    def _step_inplace(self, U: torch.Tensor, S: torch.Tensor):
+        b = self._buffers(U)
+        self._stage(0, U, U, b["ACC"], b["Ya"], S)
+        self._stage(1, U, b["Ya"], b["ACC"], b["Yb"], S)
+        self._stage(2, U, b["Yb"], b["ACC"], b["Ya"], S)
+        self._stage(3, U, b["Ya"], b["ACC"], U, S)
+
+    # ------------------------------------------------------------------
+    def rhs(self, state: BSSNState, t: float = 0.0, dt: float = None) -> BSSNState:
+        """rate = RHS + KO of ``state`` (evolve.py:86-91)."""
+        U = as_device_state(state.data if isinstance(state, BSSNState) else state)
+        dt = self.solver.dt if dt is None else dt
+        S = self._S(t, dt, U.device)
+        b = self._buffers(U)
+        rate = torch.empty_like(U)
+        self._stage(0, U, U, rate, b["Yb"], S)
+        return BSSNState(rate)
+
+    def enforce(self, state: BSSNState) -> BSSNState:
+        U = as_device_state(state.data if isinstance(state, BSSNState) else state).clone()
+        p = self.params
+        n = U[0].numel()
+        _lib.check(_lib.load().bssn_b200_enforce(_stream_handle(U.device), U.data_ptr(), n,
+                                                 p.chi_floor, p.alpha_floor))
+        return BSSNState(U)
+
+    def step(self, state: BSSNState, t: float, dt: float) -> BSSNState:
+        U = as_device_state(state.data if isinstance(state, BSSNState) else state).clone()
+        self._step_inplace(U, self._S(t, dt, U.device))
+        return BSSNState(U)
+
+    def evolve(self, state: BSSNState, dt: float, nsteps: int, t0: float = 0.0,
+               use_graph: bool = True) -> BSSNState:
+        """``nsteps`` RK4 steps from t0; the step is captured once as a CUDA graph
+        and replayed, with the time advanced on the device (t <- t + dt)."""
+        U = as_device_state(state.data if isinstance(state, BSSNState) else state).clone()
+        S = self._S(t0, dt, U.device)
+        if nsteps <= 0:
+            return BSSNState(U)
+        if not use_graph:
+            for _ in range(int(nsteps)):
+                self._step_inplace(U, S)
+                self._advance_time(S)
+            return BSSNState(U)
+        g, U_g, S_g = self.capture(U, S)
+        for _ in range(int(nsteps)):
+            g.replay()
+        U.copy_(U_g)
+        return BSSNState(U)
+
+    def capture(self, U: torch.Tensor, S: torch.Tensor):
+        """Capture one step (4 stages + time advance) on static buffers.
+        Returns (graph, U_static, S_static); replay advances U_static by one step."""
+        U_g = U.clone()
+        S_g = S.clone()
+        self._buffers(U_g)
+        Scratch.get(U_g.device)
+        side = torch.cuda.Stream(U_g.device)
+        side.wait_stream(torch.cuda.current_stream(U_g.device))
+        with torch.cuda.stream(side):
+            # warm the launch path (attributes, module load) outside the capture
+            probe_U = U_g.clone()
+            probe_S = S_g.clone()
+            self._step_inplace(probe_U, probe_S)
+        torch.cuda.current_stream(U_g.device).wait_stream(side)
+        torch.cuda.synchronize(U_g.device)
+        del probe_U, probe_S
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self._step_inplace(U_g, S_g)
+            self._advance_time(S_g)
+        return graph, U_g, S_g

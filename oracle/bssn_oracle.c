@@ -1,0 +1,497 @@
+/*
+ * TEST INFRASTRUCTURE — the CPU oracle for the BSSN right-hand side and its
+ * RK4 stage update. Only tests/, __graft_entry__.smoke() and bench.py's CPU
+ * baseline leg may load this library, and only as the checker. The product
+ * (integer-schemes_b200/) never links or calls it.
+ *
+ * It restates, in plain C and in tensor-index form, what the reference
+ * computes on this path:
+ *   - centred 6th-order first/second-derivative stencils and the 6th/8th-order
+ *     Kreiss-Oliger stencils with edge padding by the stencil's own reach
+ *       common/src/mcs_common/derivatives.py:35-49 (coefficients),
+ *       derivatives.py:78-88 (_apply: pre-scaled taps, edge pad, tap order)
+ *   - the 138-derivative bundle (mixed second derivative = first derivative
+ *     along the lower axis, then along the higher one)
+ *       3D/src/bssn3d/derivative_bundle.py:31-48
+ *   - the CAHD+SSL BSSN algebra that Dendro-GR's generated CSE evaluates
+ *       3D/src/bssn3d/vendor/bssneqs_SSL_HD_dxsq.cpp (24 outputs, lines 837-883),
+ *       written here from the BSSN equations, not from that file's statements
+ *   - Kreiss-Oliger dissipation, RK4 stages and algebraic enforcement
+ *       3D/src/bssn3d/evolve.py:76-84 (_ko), :93-119 (enforce), :125-137 (step)
+ *   - periodic ghost sync  evolve.py:65-73
+ *
+ * Parity of this restatement is pinned against the reference's own compiled
+ * algebra (oracle/_ref) and the golden fixtures in tests/golden/.
+ *
+ * Layouts are those of the C-ABI (include/bssn_b200.h): fields [24][n] in
+ * state order, derivatives [138][n], the 16-scalar pack S.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define NF 24
+#define NDERIV 138
+enum {
+  ALPHA = 0, CHI = 1, KK = 2, GT = 3, BETA = 9, AT = 12, GTI = 18, BB = 21
+};
+
+/* upper-triangular symmetric index: 00 01 02 11 12 22 */
+static const int SYM[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+static const int SYM_I[6] = {0, 0, 0, 1, 1, 2};
+static const int SYM_J[6] = {0, 1, 2, 1, 2, 2};
+
+/* the 11 fields with second derivatives, in derivative-slot order */
+static const int G2FIELDS[11] = {ALPHA, CHI, GT + 0, GT + 1, GT + 2, GT + 3,
+                                 GT + 4, GT + 5, BETA + 0, BETA + 1, BETA + 2};
+
+int oracle_g2_slot(int field) {
+  for (int m = 0; m < 11; ++m)
+    if (G2FIELDS[m] == field) return m;
+  return -1;
+}
+
+/* ------------------------------------------------------------------ */
+/* stencils                                                            */
+/* ------------------------------------------------------------------ */
+
+static const double C1_6[7] = {-1, 9, -45, 0, 45, -9, 1};       /* /60  */
+static const double C2_6[7] = {2, -27, 270, -490, 270, -27, 2}; /* /180 */
+static const double KO_6[7] = {1, -6, 15, -20, 15, -6, 1};      /* /64  */
+static const double KO_8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1}; /* /256 */
+
+static inline long clampl(long v, long lo, long hi) {
+  return v < lo ? lo : (v > hi ? hi : v);
+}
+
+/* One pass of a centred stencil along `axis` of a (Sx,Sy,Sz) array:
+ * out = sum_k (coef[k]/den*factor) * in[clamp(p + k - reach)], summed in tap
+ * order from the lowest offset, like derivatives.py:78-88. */
+static void apply_axis(const double* in, double* out, const long S[3], int axis,
+                       const double* coef, int ntap, double den, double factor) {
+  const int reach = (ntap - 1) / 2;
+  double w[9];
+  for (int k = 0; k < ntap; ++k) w[k] = (coef[k] / den) * factor;
+  const long Sx = S[0], Sy = S[1], Sz = S[2];
+  const long stride[3] = {Sy * Sz, Sz, 1};
+#pragma omp parallel for collapse(2) schedule(static)
+  for (long x = 0; x < Sx; ++x)
+    for (long y = 0; y < Sy; ++y)
+      for (long z = 0; z < Sz; ++z) {
+        const long p[3] = {x, y, z};
+        const long base = x * stride[0] + y * stride[1] + z;
+        const long pa = p[axis];
+        const long off0 = base - pa * stride[axis];
+        double acc = 0.0;
+        for (int k = 0; k < ntap; ++k) {
+          long q = clampl(pa + k - reach, 0, S[axis] - 1);
+          acc += w[k] * in[off0 + q * stride[axis]];
+        }
+        out[base] = acc;
+      }
+}
+
+/* The 138 derivatives of a (24,Sx,Sy,Sz) state. D is [138][n]. */
+void oracle_derivatives(const double* F, long Sx, long Sy, long Sz, double dx,
+                        double dy, double dz, double* D) {
+  const long S[3] = {Sx, Sy, Sz};
+  const long n = Sx * Sy * Sz;
+  const double h[3] = {dx, dy, dz};
+  double* tmp = (double*)malloc(sizeof(double) * n);
+  for (int f = 0; f < NF; ++f)
+    for (int a = 0; a < 3; ++a)
+      apply_axis(F + f * n, D + (long)(3 * f + a) * n, S, a, C1_6, 7, 60.0,
+                 1.0 / h[a]);
+  for (int m = 0; m < 11; ++m) {
+    const double* u = F + (long)G2FIELDS[m] * n;
+    for (int p = 0; p < 6; ++p) {
+      const int i = SYM_I[p], j = SYM_J[p];
+      double* out = D + (long)(72 + 6 * m + p) * n;
+      if (i == j) {
+        apply_axis(u, out, S, i, C2_6, 7, 180.0, 1.0 / (h[i] * h[i]));
+      } else {
+        apply_axis(u, tmp, S, i, C1_6, 7, 60.0, 1.0 / h[i]);
+        apply_axis(tmp, out, S, j, C1_6, 7, 60.0, 1.0 / h[j]);
+      }
+    }
+  }
+  free(tmp);
+}
+
+/* Kreiss-Oliger dissipation summed over the three axes, for all 24 fields,
+ * added in axis order to a zero accumulator (evolve.py:76-84). ko_order 6 or 8. */
+void oracle_ko(const double* F, long Sx, long Sy, long Sz, double dx, double dy,
+               double dz, double sigma, int ko_order, double* KO) {
+  const long S[3] = {Sx, Sy, Sz};
+  const long n = Sx * Sy * Sz;
+  const double h[3] = {dx, dy, dz};
+  double* tmp = (double*)malloc(sizeof(double) * n);
+  const double* coef = ko_order == 8 ? KO_8 : KO_6;
+  const int ntap = ko_order == 8 ? 9 : 7;
+  const double den = ko_order == 8 ? 256.0 : 64.0;
+  for (int f = 0; f < NF; ++f) {
+    double* acc = KO + (long)f * n;
+    for (long q = 0; q < n; ++q) acc[q] = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      apply_axis(F + (long)f * n, tmp, S, a, coef, ntap, den, sigma / h[a]);
+      for (long q = 0; q < n; ++q) acc[q] = acc[q] + tmp[q];
+    }
+  }
+  free(tmp);
+}
+
+/* ------------------------------------------------------------------ */
+/* the pointwise BSSN algebra                                          */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+  double eta, cahd_c, dt, dx, ssl_h, ssl_sigma, t;
+  double lam[4], lamf[2];
+} params_t;
+
+static params_t unpack(const double* S) {
+  params_t p;
+  p.eta = S[0]; p.cahd_c = S[1]; p.dt = S[2]; p.dx = S[3];
+  p.ssl_h = S[4]; p.ssl_sigma = S[5]; p.t = S[6];
+  for (int i = 0; i < 4; ++i) p.lam[i] = S[7 + i];
+  p.lamf[0] = S[11]; p.lamf[1] = S[12];
+  return p;
+}
+
+/* One point. f[24] fields, d[138] derivatives, out[24] rates; H_out (may be
+ * NULL) receives the Hamiltonian constraint chi*R~ + 2/3 K^2 - A~_ij A~^ij. */
+static void point_rhs(const double* f, const double* d, const params_t* P,
+                      double* out, double* H_out) {
+#define D1(F, A) d[3 * (F) + (A)]
+#define D2(F, I, J) d[72 + 6 * oracle_g2_slot(F) + SYM[I][J]]
+  const double al = f[ALPHA], chi = f[CHI], K = f[KK];
+  double g[3][3], A[3][3], beta[3], Gt[3], Bv[3];
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) {
+      g[i][j] = f[GT + SYM[i][j]];
+      A[i][j] = f[AT + SYM[i][j]];
+    }
+    beta[i] = f[BETA + i];
+    Gt[i] = f[GTI + i];
+    Bv[i] = f[BB + i];
+  }
+  /* inverse conformal metric from the adjugate */
+  double adj[3][3];
+  adj[0][0] = g[1][1] * g[2][2] - g[1][2] * g[1][2];
+  adj[0][1] = g[0][2] * g[1][2] - g[0][1] * g[2][2];
+  adj[0][2] = g[0][1] * g[1][2] - g[0][2] * g[1][1];
+  adj[1][1] = g[0][0] * g[2][2] - g[0][2] * g[0][2];
+  adj[1][2] = g[0][1] * g[0][2] - g[0][0] * g[1][2];
+  adj[2][2] = g[0][0] * g[1][1] - g[0][1] * g[0][1];
+  adj[1][0] = adj[0][1]; adj[2][0] = adj[0][2]; adj[2][1] = adj[1][2];
+  const double det = g[0][0] * adj[0][0] + g[0][1] * adj[0][1] + g[0][2] * adj[0][2];
+  double gu[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) gu[i][j] = adj[i][j] / det;
+
+  /* Christoffel symbols: C1[k][i][j] = G~_kij, C2[k][i][j] = G~^k_ij */
+  double C1[3][3][3], C2[3][3][3], C3[3][3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        C1[k][i][j] = 0.5 * (D1(GT + SYM[k][j], i) + D1(GT + SYM[k][i], j) -
+                             D1(GT + SYM[i][j], k));
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double s = 0.0;
+        for (int l = 0; l < 3; ++l) s += gu[k][l] * C1[l][i][j];
+        C2[k][i][j] = s;
+      }
+  double CalGt[3];
+  for (int i = 0; i < 3; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) s += gu[j][k] * C2[i][j][k];
+    CalGt[i] = s;
+  }
+  double dchi[3], dal[3], dK[3], guchi[3];
+  for (int a = 0; a < 3; ++a) {
+    dchi[a] = D1(CHI, a);
+    dal[a] = D1(ALPHA, a);
+    dK[a] = D1(KK, a);
+  }
+  for (int k = 0; k < 3; ++k) {
+    double s = 0.0;
+    for (int l = 0; l < 3; ++l) s += gu[k][l] * dchi[l];
+    guchi[k] = s;
+  }
+  /* physical Christoffel symbols */
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        C3[k][i][j] = C2[k][i][j] - (0.5 / chi) * ((k == i ? dchi[j] : 0.0) +
+                                                   (k == j ? dchi[i] : 0.0) -
+                                                   g[i][j] * guchi[k]);
+  double divb = 0.0;
+  for (int i = 0; i < 3; ++i) divb += D1(BETA + i, i);
+
+  /* D_i D_j alpha (physical) */
+  double DDa[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = D2(ALPHA, i, j);
+      for (int k = 0; k < 3; ++k) s -= C3[k][i][j] * dal[k];
+      DDa[i][j] = s;
+    }
+
+  /* conformal Laplacian pieces of chi */
+  double lapchi = 0.0, sqchi = 0.0;
+  for (int l = 0; l < 3; ++l)
+    for (int m = 0; m < 3; ++m) {
+      double s = D2(CHI, l, m);
+      for (int k = 0; k < 3; ++k) s -= C2[k][l][m] * dchi[k];
+      lapchi += gu[l][m] * s;
+      sqchi += gu[l][m] * dchi[l] * dchi[m];
+    }
+
+  /* Ricci tensor R_ij = R~_ij + R^chi_ij */
+  double R[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double r = 0.0;
+      for (int l = 0; l < 3; ++l)
+        for (int m = 0; m < 3; ++m) r -= 0.5 * gu[l][m] * D2(GT + SYM[i][j], l, m);
+      for (int k = 0; k < 3; ++k)
+        r += 0.5 * (g[k][i] * D1(GTI + k, j) + g[k][j] * D1(GTI + k, i));
+      for (int k = 0; k < 3; ++k) r += 0.5 * CalGt[k] * (C1[i][j][k] + C1[j][i][k]);
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l)
+          for (int m = 0; m < 3; ++m)
+            r += gu[l][m] * (C2[k][l][i] * C1[j][k][m] + C2[k][l][j] * C1[i][k][m] +
+                             C2[k][i][m] * C1[k][l][j]);
+      double Dchi = D2(CHI, i, j);
+      for (int k = 0; k < 3; ++k) Dchi -= C2[k][i][j] * dchi[k];
+      r += (0.5 / chi) * (Dchi + g[i][j] * lapchi) -
+           (0.25 / (chi * chi)) * (dchi[i] * dchi[j] + 3.0 * g[i][j] * sqchi);
+      R[i][j] = r;
+    }
+
+  double X[3][3], trX = 0.0, trR = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      X[i][j] = al * R[i][j] - DDa[i][j];
+      trX += gu[i][j] * X[i][j];
+      trR += gu[i][j] * R[i][j];
+    }
+  double AU[3][3], AA = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k)
+        for (int l = 0; l < 3; ++l) s += gu[i][k] * gu[j][l] * A[k][l];
+      AU[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) AA += A[i][j] * AU[i][j];
+  const double H = chi * trR + (2.0 / 3.0) * K * K - AA;
+  if (H_out) *H_out = H;
+
+#define ADV(F) (beta[0] * D1(F, 0) + beta[1] * D1(F, 1) + beta[2] * D1(F, 2))
+  const double sqc = sqrt(chi);
+  out[ALPHA] = P->lam[0] * ADV(ALPHA) - 2.0 * al * K -
+               sqc * P->ssl_h * (al - sqc) *
+                   exp(-0.5 * P->t * P->t / (P->ssl_sigma * P->ssl_sigma));
+  for (int i = 0; i < 3; ++i)
+    out[BETA + i] = 0.75 * (P->lamf[0] + P->lamf[1] * al) * Bv[i] + P->lam[1] * ADV(BETA + i);
+  for (int p = 0; p < 6; ++p) {
+    const int i = SYM_I[p], j = SYM_J[p];
+    double v = ADV(GT + p);
+    for (int k = 0; k < 3; ++k) v += g[i][k] * D1(BETA + k, j) + g[j][k] * D1(BETA + k, i);
+    out[GT + p] = v - (2.0 / 3.0) * g[i][j] * divb - 2.0 * al * A[i][j];
+  }
+  out[CHI] = ADV(CHI) + (2.0 / 3.0) * chi * (al * K - divb) +
+             P->cahd_c * P->dx * P->dx * chi * H / (P->dt * (10.0 * P->dx * P->dx + 1.0));
+  for (int p = 0; p < 6; ++p) {
+    const int i = SYM_I[p], j = SYM_J[p];
+    double v = ADV(AT + p);
+    for (int k = 0; k < 3; ++k) v += A[i][k] * D1(BETA + k, j) + A[j][k] * D1(BETA + k, i);
+    v -= (2.0 / 3.0) * A[i][j] * divb;
+    v += chi * (X[i][j] - (1.0 / 3.0) * g[i][j] * trX);
+    double AgA = 0.0;
+    for (int k = 0; k < 3; ++k)
+      for (int l = 0; l < 3; ++l) AgA += A[i][k] * gu[k][l] * A[l][j];
+    v += al * (K * A[i][j] - 2.0 * AgA);
+    out[AT + p] = v;
+  }
+  double lapa = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) lapa += gu[i][j] * DDa[i][j];
+  out[KK] = ADV(KK) - chi * lapa + al * (K * K / 3.0 + AA);
+  for (int i = 0; i < 3; ++i) {
+    double v = ADV(GTI + i);
+    for (int j = 0; j < 3; ++j) v -= CalGt[j] * D1(BETA + i, j);
+    v += (2.0 / 3.0) * CalGt[i] * divb;
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k)
+        v += gu[j][k] * D2(BETA + i, j, k) + (1.0 / 3.0) * gu[i][j] * D2(BETA + k, j, k);
+    for (int j = 0; j < 3; ++j) v -= 2.0 * AU[i][j] * dal[j];
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) v += 2.0 * al * C2[i][j][k] * AU[j][k];
+    for (int j = 0; j < 3; ++j)
+      v -= al * ((3.0 / chi) * AU[i][j] * dchi[j] + (4.0 / 3.0) * gu[i][j] * dK[j]);
+    out[GTI + i] = v;
+    out[BB + i] = v - P->eta * Bv[i] + P->lam[2] * ADV(BB + i) - P->lam[3] * ADV(GTI + i);
+  }
+#undef ADV
+#undef D1
+#undef D2
+}
+
+/* Pointwise algebra over n points. F [24][n], D [138][n], OUT [24][n]. */
+void oracle_rhs_algebra(long n, const double* F, const double* D, const double* S,
+                        double* OUT, double* H) {
+  const params_t P = unpack(S);
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) {
+    double f[NF], d[NDERIV], o[NF], h;
+    for (int k = 0; k < NF; ++k) f[k] = F[(long)k * n + q];
+    for (int k = 0; k < NDERIV; ++k) d[k] = D[(long)k * n + q];
+    point_rhs(f, d, &P, o, &h);
+    for (int k = 0; k < NF; ++k) OUT[(long)k * n + q] = o[k];
+    if (H) H[q] = h;
+  }
+}
+
+/* Full right-hand side of a (24,Sx,Sy,Sz) state: bundle + algebra. */
+void oracle_rhs(const double* F, long Sx, long Sy, long Sz, const double* S,
+                double* OUT) {
+  const long n = Sx * Sy * Sz;
+  double* D = (double*)malloc(sizeof(double) * NDERIV * n);
+  oracle_derivatives(F, Sx, Sy, Sz, S[13], S[14], S[15], D);
+  oracle_rhs_algebra(n, F, D, S, OUT, NULL);
+  free(D);
+}
+
+/* Hamiltonian constraint field of a state (same derivatives as the RHS). */
+void oracle_hamiltonian(const double* F, long Sx, long Sy, long Sz, double dx,
+                        double dy, double dz, double* H) {
+  const long n = Sx * Sy * Sz;
+  double* D = (double*)malloc(sizeof(double) * NDERIV * n);
+  double* OUT = (double*)malloc(sizeof(double) * NF * n);
+  double S[16] = {2.0, 0.0, 1.0, dx, 0.0, 1.0, 0.0, 1, 1, 1, 1, 1, 0, dx, dy, dz};
+  oracle_derivatives(F, Sx, Sy, Sz, dx, dy, dz, D);
+  oracle_rhs_algebra(n, F, D, S, OUT, H);
+  free(D);
+  free(OUT);
+}
+
+/* ------------------------------------------------------------------ */
+/* time integration                                                    */
+/* ------------------------------------------------------------------ */
+
+/* Algebraic enforcement in place (evolve.py:93-119). */
+void oracle_enforce(double* F, long n, double chi_floor, double alpha_floor) {
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) {
+    double g[6], a[6];
+    for (int k = 0; k < 6; ++k) {
+      g[k] = F[(long)(GT + k) * n + q];
+      a[k] = F[(long)(AT + k) * n + q];
+    }
+    const double det = g[0] * (g[3] * g[5] - g[4] * g[4]) - g[1] * (g[1] * g[5] - g[4] * g[2]) +
+                       g[2] * (g[1] * g[4] - g[3] * g[2]);
+    const double scale = pow(det, -1.0 / 3.0);
+    for (int k = 0; k < 6; ++k) g[k] = g[k] * scale;
+    const double iuxx = g[3] * g[5] - g[4] * g[4];
+    const double iuxy = g[2] * g[4] - g[1] * g[5];
+    const double iuxz = g[1] * g[4] - g[2] * g[3];
+    const double iuyy = g[0] * g[5] - g[2] * g[2];
+    const double iuyz = g[1] * g[2] - g[0] * g[4];
+    const double iuzz = g[0] * g[3] - g[1] * g[1];
+    const double trA = iuxx * a[0] + iuyy * a[3] + iuzz * a[5] +
+                       2.0 * (iuxy * a[1] + iuxz * a[2] + iuyz * a[4]);
+    const double third = trA / 3.0;
+    for (int k = 0; k < 6; ++k) {
+      F[(long)(GT + k) * n + q] = g[k];
+      F[(long)(AT + k) * n + q] = a[k] - g[k] * third;
+    }
+    double c = F[(long)CHI * n + q], al = F[(long)ALPHA * n + q];
+    F[(long)CHI * n + q] = c > chi_floor ? c : (c < chi_floor ? chi_floor : c);
+    F[(long)ALPHA * n + q] = al > alpha_floor ? al : (al < alpha_floor ? alpha_floor : al);
+  }
+}
+
+/* Periodic ghost sync in place (evolve.py:65-73), axis by axis. */
+void oracle_periodic_sync(double* F, long Sx, long Sy, long Sz, int ng) {
+  const long S[3] = {Sx, Sy, Sz};
+  const long stride[3] = {Sy * Sz, Sz, 1};
+  const long n = Sx * Sy * Sz;
+  for (int axis = 0; axis < 3; ++axis)
+    for (int f = 0; f < NF; ++f) {
+      double* u = F + (long)f * n;
+      for (long x = 0; x < Sx; ++x)
+        for (long y = 0; y < Sy; ++y)
+          for (long z = 0; z < Sz; ++z) {
+            const long p[3] = {x, y, z};
+            const long c = p[axis];
+            long src = -1;
+            if (c < ng) src = c + S[axis] - 2 * ng;
+            else if (c >= S[axis] - ng) src = c - S[axis] + 2 * ng;
+            if (src < 0) continue;
+            const long base = x * stride[0] + y * stride[1] + z - c * stride[axis];
+            u[base + c * stride[axis]] = u[base + src * stride[axis]];
+          }
+    }
+}
+
+/* rate = RHS(state) + KO(state), with optional periodic sync of the stage
+ * input first (evolve.py:86-91). */
+static void stage_rate(const double* U, long Sx, long Sy, long Sz, const double* S,
+                       double ko_sigma, int ko_order, int periodic, int ng,
+                       double* rate, double* work) {
+  const long n = Sx * Sy * Sz;
+  const double* src = U;
+  if (periodic) {
+    memcpy(work, U, sizeof(double) * NF * n);
+    oracle_periodic_sync(work, Sx, Sy, Sz, ng);
+    src = work;
+  }
+  oracle_rhs(src, Sx, Sy, Sz, S, rate);
+  if (ko_sigma > 0.0) {
+    double* ko = (double*)malloc(sizeof(double) * NF * n);
+    oracle_ko(src, Sx, Sy, Sz, S[13], S[14], S[15], ko_sigma, ko_order, ko);
+    for (long q = 0; q < NF * n; ++q) rate[q] = rate[q] + ko[q];
+    free(ko);
+  }
+}
+
+/* One RK4 step of BSSNEvolution.step (evolve.py:125-137) + enforce.
+ * S carries dt (S[2]) and the step's start time t (S[6]); each stage uses its
+ * own time and the full dt. U_out may alias nothing. */
+void oracle_rk4_step(const double* U, long Sx, long Sy, long Sz, const double* S_in,
+                     double ko_sigma, int ko_order, int periodic, int ng,
+                     double chi_floor, double alpha_floor, double* U_out) {
+  const long n = Sx * Sy * Sz;
+  const long N = NF * n;
+  double S[16];
+  memcpy(S, S_in, sizeof(S));
+  const double dt = S[2], t = S[6];
+  double* k[4];
+  for (int i = 0; i < 4; ++i) k[i] = (double*)malloc(sizeof(double) * N);
+  double* Y = (double*)malloc(sizeof(double) * N);
+  double* work = (double*)malloc(sizeof(double) * N);
+  const double c[4] = {0.0, 0.5, 0.5, 1.0};
+  for (int s = 0; s < 4; ++s) {
+    const double* in = U;
+    if (s > 0) {
+      const double h = (s == 3 ? 1.0 : 0.5) * dt;
+      for (long q = 0; q < N; ++q) Y[q] = U[q] + h * k[s - 1][q];
+      in = Y;
+    }
+    S[6] = t + c[s] * dt;
+    stage_rate(in, Sx, Sy, Sz, S, ko_sigma, ko_order, periodic, ng, k[s], work);
+  }
+  const double w = dt / 6.0;
+  for (long q = 0; q < N; ++q)
+    U_out[q] = U[q] + w * (k[0][q] + 2.0 * k[1][q] + 2.0 * k[2][q] + k[3][q]);
+  oracle_enforce(U_out, n, chi_floor, alpha_floor);
+  for (int i = 0; i < 4; ++i) free(k[i]);
+  free(Y);
+  free(work);
+}
