@@ -381,6 +381,102 @@ void oracle_hamiltonian(const double* F, long Sx, long Sy, long Sz, double dx,
   free(OUT);
 }
 
+
+/* Hamiltonian and momentum constraints at one point, the definitions of the
+ * reference's ConstraintSolver (3D/src/bssn3d/constraints.py:38-62, from
+ * Dendro-GR's physcon CSE):
+ *   H   = chi R~ + 2/3 K^2 - A~_ij A~^ij      (R~ with the metric-computed G~^k)
+ *   M_i = g~^jk (d_j A~_ki - G~^m_ji A~_km) - Gt^j A~_ij
+ *         - 3/2 g~^jk A~_ki d_j chi / chi - 2/3 d_i K   (Gt^j the evolved field) */
+static void point_constraints(const double* f, const double* d, double* H, double* M) {
+  params_t P;
+  memset(&P, 0, sizeof(P));
+  P.dt = 1.0; P.ssl_sigma = 1.0;
+  double out[NF];
+  point_rhs(f, d, &P, out, H);
+  double g[3][3], A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      g[i][j] = f[GT + SYM[i][j]];
+      A[i][j] = f[AT + SYM[i][j]];
+    }
+  double adj[3][3];
+  adj[0][0] = g[1][1] * g[2][2] - g[1][2] * g[1][2];
+  adj[0][1] = g[0][2] * g[1][2] - g[0][1] * g[2][2];
+  adj[0][2] = g[0][1] * g[1][2] - g[0][2] * g[1][1];
+  adj[1][1] = g[0][0] * g[2][2] - g[0][2] * g[0][2];
+  adj[1][2] = g[0][1] * g[0][2] - g[0][0] * g[1][2];
+  adj[2][2] = g[0][0] * g[1][1] - g[0][1] * g[0][1];
+  adj[1][0] = adj[0][1]; adj[2][0] = adj[0][2]; adj[2][1] = adj[1][2];
+  const double det = g[0][0] * adj[0][0] + g[0][1] * adj[0][1] + g[0][2] * adj[0][2];
+  double gu[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) gu[i][j] = adj[i][j] / det;
+#define D1C(F, A) d[3 * (F) + (A)]
+  double C1[3][3][3], C2[3][3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j)
+        C1[k][i][j] = 0.5 * (D1C(GT + SYM[k][j], i) + D1C(GT + SYM[k][i], j) - D1C(GT + SYM[i][j], k));
+  for (int k = 0; k < 3; ++k)
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) {
+        double s = 0.0;
+        for (int l = 0; l < 3; ++l) s += gu[k][l] * C1[l][i][j];
+        C2[k][i][j] = s;
+      }
+  const double chi = f[CHI];
+  for (int i = 0; i < 3; ++i) {
+    double m = 0.0;
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) {
+        double s = D1C(AT + SYM[k][i], j);
+        for (int mm = 0; mm < 3; ++mm) s -= C2[mm][j][i] * A[k][mm];
+        m += gu[j][k] * s;
+      }
+    for (int j = 0; j < 3; ++j) m -= f[GTI + j] * A[i][j];
+    double c = 0.0;
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) c += gu[j][k] * A[k][i] * D1C(CHI, j) / chi;
+    m -= 1.5 * c;
+    m -= (2.0 / 3.0) * D1C(KK, i);
+    M[i] = m;
+  }
+#undef D1C
+}
+
+/* Constraint fields of a state: H [n], M [3][n]. */
+void oracle_constraints(const double* F, long Sx, long Sy, long Sz, double dx, double dy,
+                        double dz, double* H, double* M) {
+  const long n = Sx * Sy * Sz;
+  double* D = (double*)malloc(sizeof(double) * NDERIV * n);
+  oracle_derivatives(F, Sx, Sy, Sz, dx, dy, dz, D);
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) {
+    double f[NF], d[NDERIV], h, m[3];
+    for (int k = 0; k < NF; ++k) f[k] = F[(long)k * n + q];
+    for (int k = 0; k < NDERIV; ++k) d[k] = D[(long)k * n + q];
+    point_constraints(f, d, &h, m);
+    H[q] = h;
+    for (int i = 0; i < 3; ++i) M[(long)i * n + q] = m[i];
+  }
+  free(D);
+}
+
+/* Pointwise constraints from supplied derivatives (for pinning against the
+ * reference's compiled physcon block). */
+void oracle_constraints_algebra(long n, const double* F, const double* D, double* H, double* M) {
+#pragma omp parallel for schedule(static)
+  for (long q = 0; q < n; ++q) {
+    double f[NF], d[NDERIV], h, m[3];
+    for (int k = 0; k < NF; ++k) f[k] = F[(long)k * n + q];
+    for (int k = 0; k < NDERIV; ++k) d[k] = D[(long)k * n + q];
+    point_constraints(f, d, &h, m);
+    H[q] = h;
+    for (int i = 0; i < 3; ++i) M[(long)i * n + q] = m[i];
+  }
+}
+
 /* ------------------------------------------------------------------ */
 /* time integration                                                    */
 /* ------------------------------------------------------------------ */

@@ -56,14 +56,37 @@ def lib():
         L.oracle_rhs.argtypes = [_P, _L, _L, _L, _P, _P]
         L.oracle_hamiltonian.argtypes = [_P, _L, _L, _L, _D, _D, _D, _P]
         L.oracle_enforce.argtypes = [_P, _L, _D, _D]
+        L.oracle_constraints.argtypes = [_P, _L, _L, _L, _D, _D, _D, _P, _P]
+        L.oracle_constraints_algebra.argtypes = [_L, _P, _P, _P, _P]
         L.oracle_periodic_sync.argtypes = [_P, _L, _L, _L, _I]
         L.oracle_rk4_step.argtypes = [_P, _L, _L, _L, _P, _D, _I, _I, _I, _D, _D, _P]
         _lib = L
     return _lib
 
 
+PHYSCON_PATH = HERE / "_ref" / "libdendro_physcon.so"
+_physcon = None
+
+
 def have_ref() -> bool:
     return REF_PATH.exists()
+
+
+def have_physcon() -> bool:
+    return PHYSCON_PATH.exists()
+
+
+def physcon_lib():
+    """The reference's compiled constraint block (``oracle/_ref``)."""
+    global _physcon
+    if _physcon is None:
+        if not PHYSCON_PATH.exists():
+            raise FileNotFoundError(f"{PHYSCON_PATH} not built: run `make -C oracle ref`")
+        L = ctypes.CDLL(str(PHYSCON_PATH))
+        L.dendro_ref_constraints.argtypes = [_L, _P, _P, _P, _P, _I]
+        L.dendro_ref_constraints.restype = _I
+        _physcon = L
+    return _physcon
 
 
 def ref_lib():
@@ -143,6 +166,46 @@ def hamiltonian(F: np.ndarray, dx, dy, dz) -> np.ndarray:
     H = np.empty((Sx, Sy, Sz))
     lib().oracle_hamiltonian(_ptr(F), Sx, Sy, Sz, dx, dy, dz, _ptr(H))
     return H
+
+
+def constraints(F: np.ndarray, dx, dy, dz):
+    """(H, M) fields of a state: H (Sx,Sy,Sz), M (3,Sx,Sy,Sz)."""
+    F = _c(F)
+    _, Sx, Sy, Sz = F.shape
+    H = np.empty((Sx, Sy, Sz))
+    M = np.empty((3, Sx, Sy, Sz))
+    lib().oracle_constraints(_ptr(F), Sx, Sy, Sz, dx, dy, dz, _ptr(H), _ptr(M))
+    return H, M
+
+
+def constraints_algebra(F: np.ndarray, D: np.ndarray):
+    F = _c(F)
+    D = _c(D)
+    n = int(np.prod(F.shape[1:]))
+    H = np.empty(F.shape[1:])
+    M = np.empty((3,) + F.shape[1:])
+    lib().oracle_constraints_algebra(n, _ptr(F), _ptr(D), _ptr(H), _ptr(M))
+    return H, M
+
+
+def ref_constraints_algebra(F: np.ndarray, D: np.ndarray, nthreads: int = 1):
+    """The reference's compiled constraints on the same inputs."""
+    F = _c(F)
+    D = _c(D)
+    n = int(np.prod(F.shape[1:]))
+    H = np.empty(F.shape[1:])
+    M = np.empty((3,) + F.shape[1:])
+    physcon_lib().dendro_ref_constraints(n, _ptr(F), _ptr(D), _ptr(H), _ptr(M), nthreads)
+    return H, M
+
+
+def constraint_norms(F: np.ndarray, dx, dy, dz, ng: int):
+    """Interior L2 norms (H, |M|) of 3D/src/bssn3d/constraints.py:53-62."""
+    H, M = constraints(F, dx, dy, dz)
+    sl = (slice(ng, -ng),) * 3
+    h = H[sl]
+    m = M[(slice(None),) + sl]
+    return float(np.sqrt(np.mean(h ** 2))), float(np.sqrt(np.mean((m ** 2).sum(axis=0))))
 
 
 def enforce(F: np.ndarray, chi_floor=1e-4, alpha_floor=1e-4) -> np.ndarray:
