@@ -250,7 +250,6 @@ def bench_b200(args):
     from bssn3d_b200 import initial_data as ID
     from bssn3d_b200.evolve import BSSNEvolution
     from bssn3d_b200.state import BSSNState
-    from bssn3d_b200.fused_rhs import Scratch
 
     grid, U_host, dt = ID.workload(1, n=args.n)
     interior = grid.interior_points

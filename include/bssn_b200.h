@@ -21,9 +21,8 @@
  * Stencils are evaluated on every point of the padded array with the index
  * clamped at the array ends, like 3D/src/bssn3d/derivative_bundle.py:31-48.
  *
- * Scratch: the fused kernels stage derivatives in a caller-provided device
- * buffer of bssn_b200_scratch_bytes() bytes (no allocation inside). Calls
- * that share one scratch buffer must be ordered on one stream.
+ * Ownership: the caller owns every buffer. No entry point allocates or frees
+ * device memory or synchronises the stream; kernels are only enqueued.
  */
 #ifndef BSSN_B200_H
 #define BSSN_B200_H
@@ -34,20 +33,29 @@
 extern "C" {
 #endif
 
+/* One block of a batched (AMR) block list. Blocks are stored back to back in
+ * one pooled buffer: block b's field f starts at double offset + f*sx*sy*sz
+ * and is a C-order (sx, sy, sz) array, the single-grid layout repeated. */
+typedef struct bssn_b200_block {
+  long long offset; /* first double of the block in the pooled state */
+  int sx, sy, sz;   /* padded extents (ghosts included) */
+  int tile0;        /* first tile of the block, filled by bssn_b200_batch_plan */
+  double h[3];      /* grid spacing dx, dy, dz */
+} bssn_b200_block;
+
+/* Tile-shape variants of the batched kernels (the autotuner's search space):
+ * 0 = 4x4x16, 1 = 2x8x16, 2 = 4x8x8, 3 = 8x4x8 points (x, y, z). */
+#define BSSN_B200_NVARIANTS 4
+
 #define BSSN_B200_OK 0
 #define BSSN_B200_EINVAL 1   /* bad shape, pointer, order or stage */
-#define BSSN_B200_ESCRATCH 2 /* scratch buffer missing or too small */
 #define BSSN_B200_ECUDA 3    /* a CUDA call or launch failed */
 
 /* Message for the last non-zero status returned on this host thread. */
 const char* bssn_b200_last_error(void);
 
-/* Library version, e.g. "bssn_b200 0.1 sm_100a". */
+/* Library version, e.g. "bssn_b200 0.2 sm_100a". */
 const char* bssn_b200_version(void);
-
-/* Bytes of device scratch the fused kernels need on the current device.
- * Independent of the grid shape (the kernels are persistent); ko_order 6 or 8. */
-size_t bssn_b200_scratch_bytes(int ko_order);
 
 /* The BSSN right-hand side: OUT = RHS(F) on every point of the padded grid.
  * Drop-in for the reference's fused FFI handler FusedImpl
@@ -56,8 +64,52 @@ size_t bssn_b200_scratch_bytes(int ko_order);
  * semantics (enqueue only, no host sync), same errors for a bad F shape or
  * scalar count. `stream` is a cudaStream_t (NULL = legacy default stream). */
 int bssn_b200_rhs(void* stream, const double* F, const double* S, double* OUT,
-                  long long Sx, long long Sy, long long Sz, void* scratch,
-                  size_t scratch_bytes);
+                  long long Sx, long long Sy, long long Sz);
+
+/* Hamiltonian and momentum constraints of F into OUT (4, Sx, Sy, Sz) = H, M0,
+ * M1, M2, with the definitions of the reference's ConstraintSolver
+ * (3D/src/bssn3d/constraints.py:38-51, Dendro-GR physcon.cpp) on the same
+ * 6th-order derivatives; S supplies dx, dy, dz (S[13..15]). */
+int bssn_b200_constraints(void* stream, const double* F, const double* S, double* OUT,
+                          long long Sx, long long Sy, long long Sz);
+
+/* Device scratch (bytes) bssn_b200_constraint_norms needs on the current
+ * device: one pair of partial sums per CTA of its persistent grid. */
+size_t bssn_b200_norms_scratch_bytes(void);
+
+/* Interior L2 norms of the constraints, ConstraintSolver.l2
+ * (3D/src/bssn3d/constraints.py:53-62): OUT2[0] = sqrt(mean(H^2)),
+ * OUT2[1] = sqrt(mean(M0^2 + M1^2 + M2^2)) over [ng, S-ng)^3, written to
+ * device memory without materialising H or M. One fused launch accumulates
+ * per-CTA partial sums in `scratch` (caller-provided, at least
+ * bssn_b200_norms_scratch_bytes()), a second launch adds them in a fixed
+ * order, so the result is bit-reproducible run to run. */
+int bssn_b200_constraint_norms(void* stream, const double* F, const double* S, long long Sx,
+                               long long Sy, long long Sz, int ng, double* scratch,
+                               size_t scratch_bytes, double* OUT2);
+
+/* Host-side plan of a block list for tile variant `variant`: fills each
+ * block's tile0 (prefix of tile counts) in the HOST table and returns the
+ * total tile count, or -1 (with bssn_b200_last_error) on a bad table. Upload
+ * the filled table to the device for the batched calls below. */
+int bssn_b200_batch_plan(bssn_b200_block* host_blocks, int nblocks, int variant);
+
+/* Batched forms of bssn_b200_rhs / bssn_b200_rk4_stage over a block list:
+ * ONE persistent launch covers every block (one CTA per SM walking the global
+ * tile list); each block is differentiated on its own padded array with its
+ * own spacing h (S[13..15] and S[3] are taken from the block, the other
+ * scalars from S). `blocks` is the planned table in DEVICE memory, `ntiles`
+ * the value bssn_b200_batch_plan returned for the same variant. The pooled
+ * buffers share the table's offsets. No 3D/src/bssn3d counterpart: the
+ * reference has no BSSN AMR (3D/src/mcs3d/amr/__init__.py:1); the block pool
+ * follows the 2D MCS AMR block pools (2D/src/mcs2d/amr/state.py:77). */
+int bssn_b200_batch_rhs(void* stream, const double* F, const double* S, double* OUT,
+                        const bssn_b200_block* blocks, int nblocks, int ntiles, int variant);
+int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const double* Y,
+                              double* ACC, double* YNEXT, const double* S, double ko_sigma,
+                              int ko_order, double chi_floor, double alpha_floor,
+                              const bssn_b200_block* blocks, int nblocks, int ntiles,
+                              int variant);
 
 /* One RK4 stage of BSSNEvolution.step (3D/src/bssn3d/evolve.py:125-137) with
  * the Kreiss-Oliger pass of evolve.py:76-84 and, after stage 3, the
@@ -69,12 +121,11 @@ int bssn_b200_rhs(void* stream, const double* F, const double* S, double* OUT,
  *   stage 3: YNEXT = enforce(U + (dt/6)*(ACC + rate))
  * S[2] = dt and S[6] = t, the step's start time. ko_sigma <= 0 disables KO.
  * YNEXT must not alias Y (other tiles still read Y's halo); it may alias U
- * at stage 3. Y may alias U at stage 0. */
+ * at stage 3. Y may alias U at stage 0. ACC aliases nothing. */
 int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* Y,
                         double* ACC, double* YNEXT, const double* S, double ko_sigma,
                         int ko_order, double chi_floor, double alpha_floor,
-                        long long Sx, long long Sy, long long Sz, void* scratch,
-                        size_t scratch_bytes);
+                        long long Sx, long long Sy, long long Sz);
 
 /* The 138 derivatives of F (and, when ko_sigma > 0, the 24 Kreiss-Oliger sums
  * after them) into DOUT (138 or 162, Sx, Sy, Sz): the derivative bundle of

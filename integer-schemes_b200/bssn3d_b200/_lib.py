@@ -14,7 +14,8 @@ from pathlib import Path
 LIB_PATH = Path(__file__).resolve().parent / "libbssn_b200.so"
 HEADER = Path(__file__).resolve().parents[2] / "include" / "bssn_b200.h"
 
-OK, EINVAL, ESCRATCH, ECUDA = 0, 1, 2, 3
+OK, EINVAL, ECUDA = 0, 1, 3
+NVARIANTS = 4  # BSSN_B200_NVARIANTS
 
 _P = ctypes.c_void_p
 _LL = ctypes.c_longlong
@@ -25,9 +26,14 @@ _SZ = ctypes.c_size_t
 _SIGNATURES = {
     "bssn_b200_last_error": ([], ctypes.c_char_p),
     "bssn_b200_version": ([], ctypes.c_char_p),
-    "bssn_b200_scratch_bytes": ([_I], _SZ),
-    "bssn_b200_rhs": ([_P, _P, _P, _P, _LL, _LL, _LL, _P, _SZ], _I),
-    "bssn_b200_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _LL, _LL, _LL, _P, _SZ], _I),
+    "bssn_b200_rhs": ([_P, _P, _P, _P, _LL, _LL, _LL], _I),
+    "bssn_b200_constraints": ([_P, _P, _P, _P, _LL, _LL, _LL], _I),
+    "bssn_b200_norms_scratch_bytes": ([], _SZ),
+    "bssn_b200_constraint_norms": ([_P, _P, _P, _LL, _LL, _LL, _I, _P, _SZ, _P], _I),
+    "bssn_b200_batch_plan": ([_P, _I, _I], _I),
+    "bssn_b200_batch_rhs": ([_P, _P, _P, _P, _P, _I, _I, _I], _I),
+    "bssn_b200_batch_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _P, _I, _I, _I], _I),
+    "bssn_b200_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _LL, _LL, _LL], _I),
     "bssn_b200_derivatives": ([_P, _P, _P, _P, _D, _I, _LL, _LL, _LL], _I),
     "bssn_b200_advance_time": ([_P, _P], _I),
     "bssn_b200_rhs_algebra": ([_P, _P, _P, _P, _P, _LL], _I),

@@ -15,7 +15,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .fused_rhs import Scratch, _stream_handle, as_device_state, device_scalars, scalars
+from .fused_rhs import _stream_handle, as_device_state, device_scalars, scalars
 from .grid import Grid
 from .rhs import BSSNSolver
 from .state import BSSNState, PhysicsParams
@@ -58,7 +58,6 @@ class BSSNEvolution:
 
     def _stage(self, stage, U, Y, ACC, YNEXT, S):
         lib = _lib.load()
-        scratch = Scratch.get(U.device)
         _, Sx, Sy, Sz = U.shape
         src = Y
         if self.bc == "periodic":
@@ -71,7 +70,7 @@ class BSSNEvolution:
         rc = lib.bssn_b200_rk4_stage(_stream_handle(U.device), stage, U.data_ptr(), src.data_ptr(),
                                      ACC.data_ptr(), YNEXT.data_ptr(), S.data_ptr(),
                                      self.ko_sigma, self.ko_order, p.chi_floor, p.alpha_floor,
-                                     Sx, Sy, Sz, scratch.data_ptr(), scratch.numel() * 8)
+                                     Sx, Sy, Sz)
         _lib.check(rc)
 
     def _advance_time(self, S: torch.Tensor):
@@ -133,7 +132,6 @@ class BSSNEvolution:
         U_g = U.clone()
         S_g = S.clone()
         self._buffers(U_g)
-        Scratch.get(U_g.device)
         side = torch.cuda.Stream(U_g.device)
         side.wait_stream(torch.cuda.current_stream(U_g.device))
         with torch.cuda.stream(side):

@@ -11,7 +11,7 @@ device); the kernel is enqueued on torch's current stream.
 
 from __future__ import annotations
 
-from typing import Dict, Mapping
+from typing import Mapping
 
 import numpy as np
 import torch
@@ -36,25 +36,6 @@ def scalars(p, dx, dy, dz, dt, t) -> np.ndarray:
 
 def _stream_handle(device) -> int:
     return torch.cuda.current_stream(device).cuda_stream
-
-
-class Scratch:
-    """The fused kernels' device scratch slab, one per device, grown on demand."""
-
-    _bufs: Dict[int, torch.Tensor] = {}
-
-    @classmethod
-    def get(cls, device: torch.device) -> torch.Tensor:
-        idx = device.index if device.index is not None else torch.cuda.current_device()
-        with torch.cuda.device(idx):
-            need = int(_lib.load().bssn_b200_scratch_bytes(8))
-            if need == 0:
-                _lib.check(_lib.ECUDA)
-            buf = cls._bufs.get(idx)
-            if buf is None or buf.numel() * 8 < need:
-                buf = torch.empty((need + 7) // 8, dtype=torch.float64, device=f"cuda:{idx}")
-                cls._bufs[idx] = buf
-        return buf
 
 
 def as_device_state(F, device=None) -> torch.Tensor:
@@ -91,12 +72,10 @@ def rhs_tensor(Fs: torch.Tensor, S_dev: torch.Tensor, out: torch.Tensor = None) 
     lib = _lib.load()
     if out is None:
         out = torch.empty_like(Fs)
-    scratch = Scratch.get(Fs.device)
     _, Sx, Sy, Sz = Fs.shape
     with torch.cuda.device(Fs.device):
         rc = lib.bssn_b200_rhs(_stream_handle(Fs.device), Fs.data_ptr(), S_dev.data_ptr(),
-                               out.data_ptr(), Sx, Sy, Sz, scratch.data_ptr(),
-                               scratch.numel() * 8)
+                               out.data_ptr(), Sx, Sy, Sz)
     _lib.check(rc)
     return out
 

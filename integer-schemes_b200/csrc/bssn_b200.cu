@@ -1,57 +1,75 @@
 // bssn_b200 — fused BSSN right-hand side and RK4 stage kernels for sm_100a,
 // behind the C ABI of include/bssn_b200.h.
 //
-// One persistent kernel per RHS evaluation. Each CTA takes 4x4x16-point tiles
-// of the padded grid in turn; per tile it
-//   1. stages each of the 24 fields' haloed tile in shared memory
-//      (cp.async, double-buffered: field f+1 streams in while field f is
-//      differentiated) and writes the 138 derivatives (+24 Kreiss-Oliger
-//      sums) of its own point to a per-CTA scratch slab that stays in L2,
-//   2. runs the register-scheduled BSSN algebra (algebra.cuh), reading the
-//      derivatives of its point back from the slab at their point of use,
-//   3. finishes in an epilogue that either stores the RHS or performs the
-//      RK4 stage update (with algebraic enforcement fused into stage 3).
+// One persistent kernel per RHS evaluation (stream_kernel). Each 256-thread CTA
+// takes 4x4x16-point tiles of the padded grid in turn, one point per thread.
+// Per tile it walks the 24 fields in the order of stream.cuh: cp.async stages
+// the field's haloed tile in shared memory (double-buffered, the next field
+// streams in while this one is differentiated), every thread takes its
+// point's axial taps once and forms the first derivative, the diagonal second
+// derivative and the Kreiss-Oliger term from them, the mixed second
+// derivatives come out of two separable passes through shared memory, and the
+// result is consumed at once by the point's BSSN accumulators (bssn::Stream).
+// No derivative is written anywhere. The epilogue stores the RHS, performs the
+// RK4 stage update (algebraic enforcement fused into stage 3) or stores the
+// constraints.
+//
 // Stencils follow 3D/src/bssn3d/derivative_bundle.py:31-48 and
 // common/src/mcs_common/derivatives.py:78-106: pre-scaled taps summed from
 // the lowest offset, index clamped at the array ends, mixed second
-// derivatives as a first derivative along the lower axis then the higher.
+// derivatives as a first derivative along the lower axis, then along the
+// higher axis of that result.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 
 #include "../../include/bssn_b200.h"
-#include "algebra.cuh"
+#include "stream.cuh"
 
 namespace bssn {
 
-constexpr int TX = 4, TY = 4, TZ = 16;
-constexpr int TILE = TX * TY * TZ;  // 256 points, one per thread
-constexpr int NTHREADS = TILE;
-constexpr int NSLOT = NDERIV + NFIELD;  // 138 derivatives + 24 KO sums
-constexpr int HZP = 24;                 // z pitch of a staged tile (16 + 2*4, 8 mod 16)
-constexpr int NSCAL = 16;
+constexpr int NTHREADS = 256;  // one point per thread, 256-point tiles
 
-enum Mode : int { MODE_DERIV = 0, MODE_RHS = 1, MODE_STAGE = 2 };
+// A tile shape X x Y x Z (Z along the contiguous axis, X*Y*Z = 256).
+template <int X_, int Y_, int Z_>
+struct Shape {
+  static constexpr int X = X_, Y = Y_, Z = Z_;
+  static_assert(X_ * Y_ * Z_ == NTHREADS, "one point per thread");
+  static_assert(Z_ >= 8 && (Z_ & (Z_ - 1)) == 0 && (Y_ & (Y_ - 1)) == 0, "power-of-two tile");
+};
+using DefaultShape = Shape<4, 4, 16>;
+
+// z pitch of staged rows: >= the row length and 8 mod 16 doubles, so the
+// 16 threads of a half-warp (one or two z rows) hit 16 distinct bank pairs.
+__host__ __device__ constexpr int zpitch(int len) { return len <= 8 ? 8 : ((len - 8 + 15) / 16) * 16 + 8; }
+
+enum Mode : int { MODE_DERIV = 0, MODE_RHS = 1, MODE_STAGE = 2, MODE_CON = 3, MODE_NORM = 4 };
 
 struct Args {
-  const double* F;      // stage input (24, n)
-  const double* U;      // u_n (stage mode)
-  double* ACC;          // accumulator (stage mode)
-  double* OUT;          // RHS (rhs mode), next stage / new state (stage mode), derivatives (deriv mode)
-  const double* S;      // 16 scalars (device)
-  double* scratch;      // per-CTA slabs [grid][NSLOT][TILE]
+  const double* F;  // stage input (24, n)
+  const double* U;  // u_n (stage mode)
+  double* ACC;      // accumulator (stage mode)
+  double* OUT;      // RHS | next stage / new state | derivatives | constraints
+  const double* S;  // 16 scalars (device)
   long long Sx, Sy, Sz, n;
   int ntx, nty, ntz;
   int stage;
   int use_ko;
   double ko_sigma;
   double chi_floor, alpha_floor;
+  int ng;             // norm mode: ghost width of the interior
+  double* partials;   // norm mode: [gridDim.x][2] per-CTA sums (scratch)
+  const bssn_b200_block* blocks;  // batched mode: block table (device), else NULL
+  int nblocks;
+  int ntiles;         // batched mode: total tiles over all blocks
 };
 
-// Stencil weights, pre-scaled on the device from S like derivatives.py:78-81.
+// Stencil weights, pre-scaled on the device from S like derivatives.py:78-81:
+// (coefficient / denominator) * factor, factor = 1/h, 1/h^2, sigma/h.
 struct Weights {
   double w1[3][7];
   double w2[3][7];
@@ -70,49 +88,120 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-template <int R>
-struct TileGeom {
-  static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HZ = TZ + 2 * R;
-  static constexpr int SX = HY * HZP, SY = HZP;
-  static constexpr int VOL = HX * HY * HZP;  // doubles per staged buffer
-  static constexpr int NELEM = HX * HY * HZ; // staged elements
-  static constexpr int PER_THREAD = (NELEM + NTHREADS - 1) / NTHREADS;
+// Compile-time loop: body(std::integral_constant<int, I>) for I = B .. E-1, so
+// that every per-field branch and register-array index is resolved statically.
+template <int B, int E>
+struct Unroll {
+  template <class Body>
+  __device__ __forceinline__ static void run(Body&& body) {
+    body(std::integral_constant<int, B>{});
+    Unroll<B + 1, E>::run(body);
+  }
+};
+template <int E>
+struct Unroll<E, E> {
+  template <class Body>
+  __device__ __forceinline__ static void run(Body&&) {}
 };
 
-// Issue the cp.async copies that stage field f's haloed tile (clamped indices).
-template <int R>
-__device__ __forceinline__ void stage_field(double* buf, const double* __restrict__ Ff,
-                                           const int (&goff)[TileGeom<R>::PER_THREAD],
-                                           const int (&soff)[TileGeom<R>::PER_THREAD]) {
-#pragma unroll
-  for (int e = 0; e < TileGeom<R>::PER_THREAD; ++e)
-    if (soff[e] >= 0) cp_async8(buf + soff[e], Ff + goff[e]);
+template <int R, class T = DefaultShape>
+struct TileGeom {
+  static constexpr int TX = T::X, TY = T::Y, TZ = T::Z;
+  static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HZ = TZ + 2 * R;
+  static constexpr int HZP = zpitch(HZ);
+  static constexpr int SX = HY * HZP, SY = HZP;
+  static constexpr int VOL = HX * HY * HZP;   // doubles per staged buffer
+  static constexpr int NELEM = HX * HY * HZ;  // staged elements
+  static constexpr int PER_THREAD = (NELEM + NTHREADS - 1) / NTHREADS;
+  // separable mixed-derivative passes
+  static constexpr int TP = zpitch(TZ + 6);                       // z pitch of T1/T2
+  static constexpr int T1Y = TY + 6, T1N = TX * T1Y * (TZ + 6);  // d/dx over y and z halos
+  static constexpr int T2N = TX * TY * (TZ + 6);                 // d/dy over the z halo
+  static constexpr int T1VOL = TX * T1Y * TP, T2VOL = TX * TY * TP;
+  static constexpr size_t SMEM = (2 * (size_t)VOL + T1VOL + T2VOL) * sizeof(double);
+};
+
+__device__ __forceinline__ Params load_params(const double* __restrict__ S) {
+  Params P;
+  P.eta = S[0]; P.cahd_c = S[1]; P.dt = S[2]; P.dx = S[3];
+  P.ssl_h = S[4]; P.ssl_sigma = S[5]; P.t = S[6];
+  P.lam0 = S[7]; P.lam1 = S[8]; P.lam2 = S[9]; P.lam3 = S[10];
+  P.lamf0 = S[11]; P.lamf1 = S[12];
+  P.hx = S[13]; P.hy = S[14]; P.hz = S[15];
+  return P;
 }
 
-// Derivatives of one field at one point from the staged tile.
 template <int R>
-__device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c, int f,
-                                             const Weights& W, bool ko, double* __restrict__ slab,
-                                             long long slot_stride) {
+__device__ __forceinline__ void init_weights(Weights& W, const double* __restrict__ S, double ko_sigma, int tid);
+
+// One axis of the weights from that axis' spacing (batched blocks carry their own).
+template <int R>
+__device__ __forceinline__ void init_weights_h(Weights& W, double h, double ko_sigma, int a) {
+  const double c1[7] = {-1, 9, -45, 0, 45, -9, 1};
+  const double c2[7] = {2, -27, 270, -490, 270, -27, 2};
+  const double k6[7] = {1, -6, 15, -20, 15, -6, 1};
+  const double k8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1};
+  const double f1 = 1.0 / h, f2 = 1.0 / (h * h), fk = ko_sigma / h;
+  for (int k = 0; k < 7; ++k) {
+    W.w1[a][k] = (c1[k] / 60.0) * f1;
+    W.w2[a][k] = (c2[k] / 180.0) * f2;
+  }
+  for (int k = 0; k < 9; ++k) W.wko[a][k] = 0.0;
+  if (R == 4)
+    for (int k = 0; k < 9; ++k) W.wko[a][k] = (k8[k] / 256.0) * fk;
+  else
+    for (int k = 0; k < 7; ++k) W.wko[a][k] = (k6[k] / 64.0) * fk;
+}
+
+template <int R>
+__device__ __forceinline__ void init_weights(Weights& W, const double* __restrict__ S, double ko_sigma, int tid) {
+  if (tid < 3) init_weights_h<R>(W, S[13 + tid], ko_sigma, tid);
+}
+
+// Issue the cp.async copies that stage one field's haloed tile, index clamped
+// at the array ends (derivatives.py:83-84 pads with the edge value).
+template <int R, class T = DefaultShape>
+__device__ __forceinline__ void stage_tile(double* buf, const double* __restrict__ Ff, long long x0,
+                                           long long y0, long long z0, long long Sx, long long Sy,
+                                           long long Sz, int tid) {
+  using Geo = TileGeom<R, T>;
+#pragma unroll
+  for (int e = 0; e < Geo::PER_THREAD; ++e) {
+    const int idx = tid + e * NTHREADS;
+    if (idx < Geo::NELEM) {
+      const int hz = idx % Geo::HZ;
+      const int hy = (idx / Geo::HZ) % Geo::HY;
+      const int hx = idx / (Geo::HZ * Geo::HY);
+      const long long qx = clampll(x0 - R + hx, Sx - 1);
+      const long long qy = clampll(y0 - R + hy, Sy - 1);
+      const long long qz = clampll(z0 - R + hz, Sz - 1);
+      cp_async8(buf + hx * Geo::SX + hy * Geo::SY + hz, Ff + (qx * Sy + qy) * Sz + qz);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Derivative bundle to global memory (the bssn_b200_derivatives entry).
+// ---------------------------------------------------------------------------
+template <int R>
+__device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c, int f, const Weights& W,
+                                             bool ko, double* __restrict__ out, long long n) {
   constexpr int st[3] = {TileGeom<R>::SX, TileGeom<R>::SY, 1};
-  // first derivatives (the zero centre tap of the 6th-order stencil is skipped)
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < 7; ++k)
       if (k != 3) acc += W.w1[a][k] * t[c + (k - 3) * st[a]];
-    slab[(long long)d1(f, a) * slot_stride] = acc;
+    out[(long long)d1slot(f, a) * n] = acc;
   }
-  const bool has2 = (f <= F_CHI) || (f >= F_GT && f < F_AT);
-  if (has2) {
-    const int m = g2slot(f);
+  if (has_d2(f)) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
       double acc = 0.0;
 #pragma unroll
       for (int k = 0; k < 7; ++k) acc += W.w2[a][k] * t[c + (k - 3) * st[a]];
-      slab[(long long)(72 + 6 * m + sym(a, a)) * slot_stride] = acc;
+      out[(long long)d2slot(f, sym(a, a)) * n] = acc;
     }
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -128,7 +217,7 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
             if (a != 3) inner += W.w1[i][a] * t[c + (a - 3) * st[i] + (b - 3) * st[j]];
           acc += W.w1[j][b] * inner;
         }
-        slab[(long long)(72 + 6 * m + sym(i, j)) * slot_stride] = acc;
+        out[(long long)d2slot(f, sym(i, j)) * n] = acc;
       }
   }
   if (ko) {
@@ -140,129 +229,229 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
       for (int k = 0; k <= 2 * R; ++k) s += W.wko[a][k] * t[c + (k - R) * st[a]];
       acc += s;
     }
-    slab[(long long)(NDERIV + f) * slot_stride] = acc;
+    out[(long long)(NDERIV + f) * n] = acc;
   }
 }
 
-__device__ __forceinline__ Params load_params(const double* __restrict__ S) {
-  Params P;
-  P.eta = S[0]; P.cahd_c = S[1]; P.dt = S[2]; P.dx = S[3];
-  P.ssl_h = S[4]; P.ssl_sigma = S[5]; P.t = S[6];
-  P.lam0 = S[7]; P.lam1 = S[8]; P.lam2 = S[9]; P.lam3 = S[10];
-  P.lamf0 = S[11]; P.lamf1 = S[12];
-  P.hx = S[13]; P.hy = S[14]; P.hz = S[15];
-  return P;
-}
-
-template <int R, int MODE>
-__global__ void __launch_bounds__(NTHREADS, 1) fused_kernel(const Args args) {
+template <int R>
+__global__ void __launch_bounds__(NTHREADS) deriv_kernel(const Args args) {
   using Geo = TileGeom<R>;
   extern __shared__ __align__(16) double smem[];
-  double* buf0 = smem;
-  double* buf1 = smem + Geo::VOL;
   __shared__ Weights W;
-
   const int tid = threadIdx.x;
-  const long long Sx = args.Sx, Sy = args.Sy, Sz = args.Sz, n = args.n;
-  if (tid < 3) {
-    const int a = tid;
-    const double h = args.S[13 + a];
-    const double c1[7] = {-1, 9, -45, 0, 45, -9, 1};
-    const double c2[7] = {2, -27, 270, -490, 270, -27, 2};
-    const double k6[7] = {1, -6, 15, -20, 15, -6, 1};
-    const double k8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1};
-    const double f1 = 1.0 / h, f2 = 1.0 / (h * h), fk = args.ko_sigma / h;
-    for (int k = 0; k < 7; ++k) {
-      W.w1[a][k] = (c1[k] / 60.0) * f1;
-      W.w2[a][k] = (c2[k] / 180.0) * f2;
-    }
-    for (int k = 0; k < 9; ++k) W.wko[a][k] = 0.0;
-    if (R == 4)
-      for (int k = 0; k < 9; ++k) W.wko[a][k] = (k8[k] / 256.0) * fk;
-    else
-      for (int k = 0; k < 7; ++k) W.wko[a][k] = (k6[k] / 64.0) * fk;
-  }
+  init_weights<R>(W, args.S, args.ko_sigma, tid);
   __syncthreads();
-
-  const int lz = tid & (TZ - 1), ly = (tid >> 4) & (TY - 1), lx = tid >> 6;
+  const long long Sx = args.Sx, Sy = args.Sy, Sz = args.Sz, n = args.n;
+  constexpr int TX = Geo::TX, TY = Geo::TY, TZ = Geo::TZ;
+  const int lz = tid % TZ, ly = (tid / TZ) % TY, lx = tid / (TZ * TY);
   const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R);
   const int ntiles = args.ntx * args.nty * args.ntz;
-  double* slab_cta = args.scratch + (long long)blockIdx.x * NSLOT * TILE;
-  const bool ko = args.use_ko != 0;
-
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int tz = tile % args.ntz;
-    const int ty = (tile / args.ntz) % args.nty;
-    const int tx = tile / (args.ntz * args.nty);
+    const int tz = tile % args.ntz, ty = (tile / args.ntz) % args.nty, tx = tile / (args.ntz * args.nty);
     const long long x0 = (long long)tx * TX, y0 = (long long)ty * TY, z0 = (long long)tz * TZ;
     const long long gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
     const bool inside = gx < Sx && gy < Sy && gz < Sz;
-    const long long gidx = (gx * Sy + gy) * Sz + gz;
+    double* out = args.OUT + (gx * Sy + gy) * Sz + gz;
+    for (int f = 0; f < NFIELD; ++f) {
+      stage_tile<R>(smem, args.F + (long long)f * n, x0, y0, z0, Sx, Sy, Sz, tid);
+      cp_async_commit();
+      cp_async_wait<0>();
+      __syncthreads();
+      if (inside) field_derivs<R>(smem, c, f, W, args.use_ko != 0, out, n);
+      __syncthreads();
+    }
+  }
+}
 
-    // per-thread staged-element offsets (the same for every field)
-    int goff[Geo::PER_THREAD], soff[Geo::PER_THREAD];
-#pragma unroll
-    for (int e = 0; e < Geo::PER_THREAD; ++e) {
-      const int idx = tid + e * NTHREADS;
-      if (idx < Geo::NELEM) {
-        const int hz = idx % Geo::HZ;
-        const int hy = (idx / Geo::HZ) % Geo::HY;
-        const int hx = idx / (Geo::HZ * Geo::HY);
-        const long long qx = clampll(x0 - R + hx, Sx - 1);
-        const long long qy = clampll(y0 - R + hy, Sy - 1);
-        const long long qz = clampll(z0 - R + hz, Sz - 1);
-        goff[e] = (int)((qx * Sy + qy) * Sz + qz);
-        soff[e] = hx * Geo::SX + hy * Geo::SY + hz;
-      } else {
-        goff[e] = 0;
-        soff[e] = -1;
+// ---------------------------------------------------------------------------
+// The streaming fused kernel.
+// ---------------------------------------------------------------------------
+template <int R, int MODE, class T = DefaultShape>
+__global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
+  using Geo = TileGeom<R, T>;
+  constexpr int TX = Geo::TX, TY = Geo::TY, TZ = Geo::TZ, HZP = Geo::TP;
+  constexpr bool RATES = MODE != MODE_CON && MODE != MODE_NORM;
+  constexpr bool CONS = MODE == MODE_CON || MODE == MODE_NORM;
+  extern __shared__ __align__(16) double smem[];
+  double* const buf0 = smem;
+  double* const buf1 = smem + Geo::VOL;
+  double* const T1 = smem + 2 * Geo::VOL;
+  double* const T2 = T1 + Geo::T1VOL;
+  __shared__ Weights W;
+
+  const int tid = threadIdx.x;
+  const bool batched = args.blocks != nullptr;
+  const int lz = tid % TZ, ly = (tid / TZ) % TY, lx = tid / (TZ * TY);
+  const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R);
+  constexpr int st[3] = {Geo::SX, Geo::SY, 1};
+  const int ntiles = batched ? args.ntiles : args.ntx * args.nty * args.ntz;
+  const bool use_ko = RATES && args.use_ko != 0;
+  const Params P0 = load_params(args.S);
+  double norm_h = 0.0, norm_m = 0.0;  // norm mode: this thread's interior sums
+  const double cs = args.stage == 0 ? 0.0 : (args.stage == 3 ? 1.0 : 0.5);
+  if (!batched) {
+    init_weights<R>(W, args.S, args.ko_sigma, tid);
+    __syncthreads();
+  }
+  int cur_block = -1;
+
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    // ---- tile geometry: the single grid, or the block that owns this tile ----
+    long long Sx = args.Sx, Sy = args.Sy, Sz = args.Sz, n = args.n, base = 0;
+    int ntx = args.ntx, nty = args.nty, ntz = args.ntz, lt = tile;
+    Params P = P0;
+    if (batched) {
+      int lo = 0, hi = args.nblocks - 1;  // last block with tile0 <= tile
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (args.blocks[mid].tile0 <= tile) lo = mid; else hi = mid - 1;
+      }
+      const bssn_b200_block bk = args.blocks[lo];
+      Sx = bk.sx; Sy = bk.sy; Sz = bk.sz;
+      n = Sx * Sy * Sz;
+      base = bk.offset;
+      ntx = (bk.sx + TX - 1) / TX; nty = (bk.sy + TY - 1) / TY; ntz = (bk.sz + TZ - 1) / TZ;
+      lt = tile - bk.tile0;
+      P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
+      if (lo != cur_block) {
+        // every thread finished the previous tile's last field step (it ends in a barrier)
+        if (tid < 3) init_weights_h<R>(W, bk.h[tid], args.ko_sigma, tid);
+        cur_block = lo;
       }
     }
+    if (MODE == MODE_STAGE) P.t = P0.t + cs * P0.dt;  // stage time t, t+dt/2, t+dt/2, t+dt (evolve.py:125-131)
+    const int tz = lt % ntz, ty = (lt / ntz) % nty, tx = lt / (ntz * nty);
+    const long long x0 = (long long)tx * TX, y0 = (long long)ty * TY, z0 = (long long)tz * TZ;
+    const long long gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
+    const bool inside = gx < Sx && gy < Sy && gz < Sz;
+    // points past the array end compute on clamped data and store nothing
+    const long long gidx = base + (clampll(gx, Sx - 1) * Sy + clampll(gy, Sy - 1)) * Sz + clampll(gz, Sz - 1);
+    const double* __restrict__ Fbase = args.F + base;
+    const double* __restrict__ Fp = args.F + gidx;
+    auto fld = [&](int k) -> double { return __ldg(Fp + (long long)k * n); };
 
-    double* slab;
-    long long slot_stride;
-    if (MODE == MODE_DERIV) {
-      slab = args.OUT + gidx;
-      slot_stride = n;
-    } else {
-      slab = slab_cta + tid;
-      slot_stride = TILE;
-    }
+    Stream<RATES, CONS> acc;
+    acc.init(fld);
 
-    // ---- phase 1: derivatives, field by field -------------------------
-    stage_field<R>(buf0, args.F, goff, soff);
+    stage_tile<R, T>(buf0, Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
     cp_async_commit();
-    for (int f = 0; f < NFIELD; ++f) {
-      double* cur = (f & 1) ? buf1 : buf0;
-      double* nxt = (f & 1) ? buf0 : buf1;
-      if (f + 1 < NFIELD) {
-        stage_field<R>(nxt, args.F + (long long)(f + 1) * n, goff, soff);
+    Unroll<0, NFIELD>::run([&](auto ic) {
+      constexpr int idx = decltype(ic)::value;
+      constexpr int f = stream_field(idx);
+      const double* __restrict__ cur = (idx & 1) ? buf1 : buf0;
+      if (idx + 1 < NFIELD) {
+        stage_tile<R, T>((idx & 1) ? buf0 : buf1, Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
+                         Sx, Sy, Sz, tid);
         cp_async_commit();
         cp_async_wait<1>();
       } else {
         cp_async_wait<0>();
       }
       __syncthreads();
-      if (inside) field_derivs<R>(cur, c, f, W, ko, slab, slot_stride);
-      __syncthreads();
-    }
-    if (MODE == MODE_DERIV || !inside) continue;
 
-    // ---- phase 2: algebra + epilogue ------------------------------------
-    Params P = load_params(args.S);
-    const double* __restrict__ Fp = args.F + gidx;
-    const double* __restrict__ sl = slab;
-    auto fld = [&](int k) -> double { return __ldg(Fp + (long long)k * n); };
-    auto drv = [&](int s) -> double { return sl[s * TILE]; };
+      // axial taps: first derivative, diagonal second derivative, KO
+      double d1[3], d2[6], ko = 0.0;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        double v[2 * R + 1];
+#pragma unroll
+        for (int k = 0; k <= 2 * R; ++k) v[k] = cur[c + (k - R) * st[a]];
+        double s1 = 0.0;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+          if (k != 3) s1 += W.w1[a][k] * v[k + R - 3];
+        d1[a] = s1;
+        if (has_d2(f)) {
+          double s2 = 0.0;
+#pragma unroll
+          for (int k = 0; k < 7; ++k) s2 += W.w2[a][k] * v[k + R - 3];
+          d2[sym(a, a)] = s2;
+        }
+        if (use_ko) {
+          double sk = 0.0;
+#pragma unroll
+          for (int k = 0; k <= 2 * R; ++k) sk += W.wko[a][k] * v[k];
+          ko += sk;
+        }
+      }
+      if (has_d2(f)) {
+        // T1 = d/dx over x in [0,TX), y in [-3, TY+3), z in [-3, TZ+3)
+        for (int e = tid; e < Geo::T1N; e += NTHREADS) {
+          const int zz = e % (TZ + 6);
+          const int yy = (e / (TZ + 6)) % Geo::T1Y;
+          const int xx = e / ((TZ + 6) * Geo::T1Y);
+          const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R);
+          double s = 0.0;
+#pragma unroll
+          for (int k = 0; k < 7; ++k)
+            if (k != 3) s += W.w1[0][k] * cur[cc + (k - 3) * Geo::SX];
+          T1[(xx * Geo::T1Y + yy) * HZP + zz] = s;
+        }
+        // T2 = d/dy over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
+        for (int e = tid; e < Geo::T2N; e += NTHREADS) {
+          const int zz = e % (TZ + 6);
+          const int yy = (e / (TZ + 6)) % TY;
+          const int xx = e / ((TZ + 6) * TY);
+          const int cc = (xx + R) * Geo::SX + (yy + R) * Geo::SY + (zz - 3 + R);
+          double s = 0.0;
+#pragma unroll
+          for (int k = 0; k < 7; ++k)
+            if (k != 3) s += W.w1[1][k] * cur[cc + (k - 3) * Geo::SY];
+          T2[(xx * TY + yy) * HZP + zz] = s;
+        }
+        __syncthreads();
+        double sxy = 0.0, sxz = 0.0, syz = 0.0;
+        const int t1c = (lx * Geo::T1Y + ly + 3) * HZP + lz + 3;
+        const int t2c = (lx * TY + ly) * HZP + lz + 3;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) {
+          if (k == 3) continue;
+          sxy += W.w1[1][k] * T1[t1c + (k - 3) * HZP];
+          sxz += W.w1[2][k] * T1[t1c + (k - 3)];
+          syz += W.w1[2][k] * T2[t2c + (k - 3)];
+        }
+        d2[sym(0, 1)] = sxy;
+        d2[sym(0, 2)] = sxz;
+        d2[sym(1, 2)] = syz;
+      } else {
+#pragma unroll
+        for (int p = 0; p < 6; ++p) d2[p] = 0.0;
+      }
+      acc.consume(f, d1, d2, ko, P, fld);
+      __syncthreads();  // staged buffer and T1/T2 are reused
+    });
+
+    // ---- epilogue ---------------------------------------------------------
     if (MODE == MODE_RHS) {
       double* O = args.OUT + gidx;
-      auto emit = [&](int k, double v) { O[(long long)k * n] = v; };
-      rhs_point(fld, drv, emit, P);
+      auto emit = [&](int k, double v) {
+        if (inside) O[(long long)k * n] = v;
+      };
+      acc.finalize(fld, P, emit, NoCon());
+    } else if (MODE == MODE_CON) {
+      double* O = args.OUT + gidx;
+      auto con = [&](double h, double m0, double m1, double m2) {
+        if (inside) {
+          O[0] = h;
+          O[n] = m0;
+          O[2 * n] = m1;
+          O[3 * n] = m2;
+        }
+      };
+      acc.finalize(fld, P, [](int, double) {}, con);
+    } else if (MODE == MODE_NORM) {
+      const int g = args.ng;
+      const bool interior = inside && gx >= g && gx < Sx - g && gy >= g && gy < Sy - g && gz >= g && gz < Sz - g;
+      auto con = [&](double h, double m0, double m1, double m2) {
+        if (interior) {
+          norm_h += h * h;
+          norm_m += m0 * m0 + m1 * m1 + m2 * m2;
+        }
+      };
+      acc.finalize(fld, P, [](int, double) {}, con);
     } else {
       const int stage = args.stage;
       const double dt = P.dt;
-      const double cs = stage == 0 ? 0.0 : (stage == 3 ? 1.0 : 0.5);
-      P.t = P.t + cs * dt;
       const double hstep = (stage == 2) ? dt : 0.5 * dt;
       const double w6 = dt / 6.0;
       const double* __restrict__ Up = args.U + gidx;
@@ -271,26 +460,29 @@ __global__ void __launch_bounds__(NTHREADS, 1) fused_kernel(const Args args) {
       double en[14];  // stage 3: gt0..5, At0..5, chi, alpha held for enforcement
 #pragma unroll
       for (int q = 0; q < 14; ++q) en[q] = 0.0;
-      auto emit = [&](int k, double v) {
-        const double rate = ko ? v + sl[(NDERIV + k) * TILE] : v;
+      auto emit = [&](int k, double rate) {
         const double u = Up[(long long)k * n];
         if (stage == 0) {
-          A[(long long)k * n] = rate;
-          O[(long long)k * n] = u + hstep * rate;
+          if (inside) {
+            A[(long long)k * n] = rate;
+            O[(long long)k * n] = u + hstep * rate;
+          }
         } else if (stage < 3) {
-          A[(long long)k * n] = A[(long long)k * n] + 2.0 * rate;
-          O[(long long)k * n] = u + hstep * rate;
+          if (inside) {
+            A[(long long)k * n] = A[(long long)k * n] + 2.0 * rate;
+            O[(long long)k * n] = u + hstep * rate;
+          }
         } else {
           const double un = u + w6 * (A[(long long)k * n] + rate);
           if (k >= F_GT && k < F_GT + 6) en[k - F_GT] = un;
           else if (k >= F_AT && k < F_AT + 6) en[6 + k - F_AT] = un;
           else if (k == F_CHI) en[12] = un;
           else if (k == F_ALPHA) en[13] = un;
-          else O[(long long)k * n] = un;
+          else if (inside) O[(long long)k * n] = un;
         }
       };
-      rhs_point(fld, drv, emit, P);
-      if (stage == 3) {
+      acc.finalize(fld, P, emit, NoCon());
+      if (stage == 3 && inside) {
         // algebraic enforcement, evolve.py:93-119
         double* g = en;
         double* a = en + 6;
@@ -317,6 +509,41 @@ __global__ void __launch_bounds__(NTHREADS, 1) fused_kernel(const Args args) {
       }
     }
   }
+  if (MODE == MODE_NORM) {
+    // fixed-order block reduction of the per-thread sums (reuses the staging buffer)
+    __syncthreads();
+    double* red = smem;
+    red[2 * tid] = norm_h;
+    red[2 * tid + 1] = norm_m;
+    __syncthreads();
+    for (int w = NTHREADS / 2; w > 0; w >>= 1) {
+      if (tid < w) {
+        red[2 * tid] += red[2 * (tid + w)];
+        red[2 * tid + 1] += red[2 * (tid + w) + 1];
+      }
+      __syncthreads();
+    }
+    if (tid == 0) {
+      args.partials[2 * blockIdx.x] = red[0];
+      args.partials[2 * blockIdx.x + 1] = red[1];
+    }
+  }
+}
+
+// Second pass of the constraint norms: the per-CTA partial sums in index
+// order (deterministic for a given grid), then RMS over the interior
+// (3D/src/bssn3d/constraints.py:53-62).
+__global__ void norm_finalize_kernel(const double* __restrict__ partials, int nparts, double count,
+                                     double* __restrict__ out) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double h = 0.0, m = 0.0;
+    for (int i = 0; i < nparts; ++i) {
+      h += partials[2 * i];
+      m += partials[2 * i + 1];
+    }
+    out[0] = sqrt(h / count);
+    out[1] = sqrt(m / count);
+  }
 }
 
 // t <- t + dt in the device scalar pack, between captured RK4 steps
@@ -326,7 +553,8 @@ __global__ void advance_time_kernel(double* S) {
 }
 
 // Algebra only: derivatives supplied by the caller (the reference's
-// algebra-only microbenchmark interface, 3D/src/bssn3d/cuda/microbench_algebra.cu).
+// algebra-only microbenchmark interface, 3D/src/bssn3d/cuda/gen_algebra_cuda.py:55-96),
+// consumed in the stream order of the fused kernel.
 __global__ void __launch_bounds__(128) algebra_kernel(const double* __restrict__ F, const double* __restrict__ D,
                                                       const double* __restrict__ S, double* __restrict__ OUT,
                                                       long long n) {
@@ -334,8 +562,19 @@ __global__ void __launch_bounds__(128) algebra_kernel(const double* __restrict__
   for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
     auto fld = [&](int k) -> double { return __ldg(F + (long long)k * n + q); };
     auto drv = [&](int s) -> double { return __ldg(D + (long long)s * n + q); };
+    Stream<true, false> acc;
+    acc.init(fld);
+    Unroll<0, NFIELD>::run([&](auto ic) {
+      constexpr int f = stream_field(decltype(ic)::value);
+      double d1[3], d2[6];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) d1[a] = drv(d1slot(f, a));
+#pragma unroll
+      for (int p = 0; p < 6; ++p) d2[p] = has_d2(f) ? drv(d2slot(f, p)) : 0.0;
+      acc.consume(f, d1, d2, 0.0, P, fld);
+    });
     auto emit = [&](int k, double v) { OUT[(long long)k * n + q] = v; };
-    rhs_point(fld, drv, emit, P);
+    acc.finalize(fld, P, emit, NoCon());
   }
 }
 
@@ -372,7 +611,6 @@ __global__ void periodic_axis_kernel(double* __restrict__ U, long long Sx, long 
   const long long S[3] = {Sx, Sy, Sz};
   const long long st[3] = {Sy * Sz, Sz, 1};
   const long long n = Sx * Sy * Sz;
-  // iterate over the 2*ng ghost layers x the other two axes x 24 fields
   const long long o1 = S[(axis + 1) % 3], o2 = S[(axis + 2) % 3];
   const long long per_field = 2LL * ng * o1 * o2;
   const long long total = per_field * NFIELD;
@@ -407,87 +645,123 @@ int cuda_fail(const char* what, cudaError_t e) {
   return fail(BSSN_B200_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
-struct DeviceInfo {
-  int device = -1;
-  int sms = 0;
-  int ctas_per_sm = 1;
-};
+constexpr int kMaxDev = 64;
 
-int device_info(DeviceInfo* out) {
+int device_sms(int* sms) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
-  static thread_local DeviceInfo cache[16];
-  if (dev >= 0 && dev < 16 && cache[dev].device == dev) {
-    *out = cache[dev];
+  static int cache[kMaxDev] = {0};
+  if (dev >= 0 && dev < kMaxDev && cache[dev] > 0) {
+    *sms = cache[dev];
     return 0;
   }
-  DeviceInfo d;
-  d.device = dev;
-  e = cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, dev);
+  int v = 0;
+  e = cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return cuda_fail("cudaDeviceGetAttribute", e);
-  d.ctas_per_sm = 1;  // __launch_bounds__(256, 1) kernels: one resident CTA per SM
-  if (dev >= 0 && dev < 16) cache[dev] = d;
-  *out = d;
+  if (dev >= 0 && dev < kMaxDev) cache[dev] = v;
+  *sms = v;
   return 0;
 }
 
-template <int R, int MODE>
-int launch_fused(const bssn::Args& a, cudaStream_t stream, int grid) {
-  using Geo = bssn::TileGeom<R>;
-  const size_t smem = 2 * (size_t)Geo::VOL * sizeof(double);
-  auto kern = bssn::fused_kernel<R, MODE>;
-  static thread_local int attr_set[16] = {0};
+// Opt a kernel into its dynamic shared memory once per device.
+template <class K>
+int set_smem(K kern, size_t smem, int* flags) {
   int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 16 && !attr_set[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  if (dev < 0 || dev >= kMaxDev) return fail(BSSN_B200_EINVAL, "device ordinal out of range");
+  if (!flags[dev]) {
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_fail("cudaFuncSetAttribute", e);
-    attr_set[dev] = 1;
+    flags[dev] = 1;
   }
+  return 0;
+}
+
+template <int R, int MODE, class T = bssn::DefaultShape>
+int launch_stream(const bssn::Args& a, cudaStream_t stream, int grid) {
+  using Geo = bssn::TileGeom<R, T>;
+  const size_t smem = Geo::SMEM;
+  auto kern = bssn::stream_kernel<R, MODE, T>;
+  static int flags[kMaxDev] = {0};
+  int rc = set_smem(kern, smem, flags);
+  if (rc) return rc;
   kern<<<grid, bssn::NTHREADS, smem, stream>>>(a);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_fail("fused kernel launch", e);
+  if (e != cudaSuccess) return cuda_fail("stream kernel launch", e);
+  return 0;
+}
+
+template <int R>
+int launch_deriv(const bssn::Args& a, cudaStream_t stream, int grid) {
+  using Geo = bssn::TileGeom<R>;
+  const size_t smem = (size_t)Geo::VOL * sizeof(double);
+  auto kern = bssn::deriv_kernel<R>;
+  static int flags[kMaxDev] = {0};
+  int rc = set_smem(kern, smem, flags);
+  if (rc) return rc;
+  kern<<<grid, bssn::NTHREADS, smem, stream>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail("derivative kernel launch", e);
   return 0;
 }
 
 int check_grid(long long Sx, long long Sy, long long Sz) {
   if (Sx < 1 || Sy < 1 || Sz < 1) return fail(BSSN_B200_EINVAL, "grid extents must be >= 1");
-  const long long n = Sx * Sy * Sz;
-  if (n > (1LL << 31) - 1) return fail(BSSN_B200_EINVAL, "grid has more than 2^31-1 points");
-  if ((long long)bssn::NFIELD * n > (1LL << 40)) return fail(BSSN_B200_EINVAL, "grid too large");
+  if (Sx > (1LL << 31) / Sy / Sz) return fail(BSSN_B200_EINVAL, "grid has more than 2^31 points");
   return 0;
 }
 
-int prepare(bssn::Args* a, long long Sx, long long Sy, long long Sz, int* grid) {
+// Fill the shape fields of `a` and the persistent grid size (one CTA per SM).
+int prepare(bssn::Args* a, long long Sx, long long Sy, long long Sz, int ctas_per_sm, int* grid) {
   int rc = check_grid(Sx, Sy, Sz);
   if (rc) return rc;
-  DeviceInfo d;
-  rc = device_info(&d);
+  int sms = 0;
+  rc = device_sms(&sms);
   if (rc) return rc;
   a->Sx = Sx; a->Sy = Sy; a->Sz = Sz;
   a->n = Sx * Sy * Sz;
-  a->ntx = (int)((Sx + bssn::TX - 1) / bssn::TX);
-  a->nty = (int)((Sy + bssn::TY - 1) / bssn::TY);
-  a->ntz = (int)((Sz + bssn::TZ - 1) / bssn::TZ);
+  using D = bssn::DefaultShape;
+  a->ntx = (int)((Sx + D::X - 1) / D::X);
+  a->nty = (int)((Sy + D::Y - 1) / D::Y);
+  a->ntz = (int)((Sz + D::Z - 1) / D::Z);
   const long long ntiles = (long long)a->ntx * a->nty * a->ntz;
-  const long long cap = (long long)d.sms * d.ctas_per_sm;
+  const long long cap = (long long)sms * ctas_per_sm;
   *grid = (int)(ntiles < cap ? ntiles : cap);
   return 0;
 }
 
-size_t scratch_for(const DeviceInfo& d) {
-  return (size_t)d.sms * d.ctas_per_sm * bssn::NSLOT * bssn::TILE * sizeof(double);
+void variant_shape(int variant, int* tx, int* ty, int* tz) {
+  static const int shapes[BSSN_B200_NVARIANTS][3] = {{4, 4, 16}, {2, 8, 16}, {4, 8, 8}, {8, 4, 8}};
+  *tx = shapes[variant][0];
+  *ty = shapes[variant][1];
+  *tz = shapes[variant][2];
 }
 
-int check_scratch(void* scratch, size_t bytes) {
-  DeviceInfo d;
-  int rc = device_info(&d);
+template <int R, int MODE>
+int launch_variant(const bssn::Args& a, cudaStream_t st, int grid, int variant) {
+  switch (variant) {
+    case 0: return launch_stream<R, MODE, bssn::Shape<4, 4, 16>>(a, st, grid);
+    case 1: return launch_stream<R, MODE, bssn::Shape<2, 8, 16>>(a, st, grid);
+    case 2: return launch_stream<R, MODE, bssn::Shape<4, 8, 8>>(a, st, grid);
+    case 3: return launch_stream<R, MODE, bssn::Shape<8, 4, 8>>(a, st, grid);
+    default: return fail(BSSN_B200_EINVAL, "variant out of range");
+  }
+}
+
+int prepare_batch(bssn::Args* a, const bssn_b200_block* blocks, int nblocks, int ntiles, int variant, int* grid) {
+  if (!blocks) return fail(BSSN_B200_EINVAL, "batch: NULL block table");
+  if (nblocks < 1) return fail(BSSN_B200_EINVAL, "batch: nblocks must be >= 1");
+  if (ntiles < 1) return fail(BSSN_B200_EINVAL, "batch: ntiles must be >= 1 (run bssn_b200_batch_plan)");
+  if (variant < 0 || variant >= BSSN_B200_NVARIANTS) return fail(BSSN_B200_EINVAL, "batch: variant out of range");
+  int sms = 0;
+  int rc = device_sms(&sms);
   if (rc) return rc;
-  if (!scratch) return fail(BSSN_B200_ESCRATCH, "scratch pointer is NULL");
-  if (bytes < scratch_for(d))
-    return fail(BSSN_B200_ESCRATCH, "scratch buffer smaller than bssn_b200_scratch_bytes()");
-  if ((reinterpret_cast<uintptr_t>(scratch) & 15) != 0) return fail(BSSN_B200_EINVAL, "scratch not 16-byte aligned");
+  a->blocks = blocks;
+  a->nblocks = nblocks;
+  a->ntiles = ntiles;
+  *grid = ntiles < sms ? ntiles : sms;
   return 0;
 }
 
@@ -495,57 +769,150 @@ int check_scratch(void* scratch, size_t bytes) {
 
 extern "C" {
 
-const char* bssn_b200_last_error(void) { return g_err.c_str(); }
-
-const char* bssn_b200_version(void) { return "bssn_b200 0.1 sm_100a"; }
-
-size_t bssn_b200_scratch_bytes(int ko_order) {
-  (void)ko_order;
-  DeviceInfo d;
-  if (device_info(&d)) return 0;
-  return scratch_for(d);
+int bssn_b200_batch_plan(bssn_b200_block* host_blocks, int nblocks, int variant) {
+  if (!host_blocks || nblocks < 1) {
+    fail(BSSN_B200_EINVAL, "batch_plan: empty block table");
+    return -1;
+  }
+  if (variant < 0 || variant >= BSSN_B200_NVARIANTS) {
+    fail(BSSN_B200_EINVAL, "batch_plan: variant out of range");
+    return -1;
+  }
+  int tx, ty, tz;
+  variant_shape(variant, &tx, &ty, &tz);
+  long long t0 = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    bssn_b200_block& bk = host_blocks[b];
+    if (bk.sx < 1 || bk.sy < 1 || bk.sz < 1 || bk.offset < 0 || !(bk.h[0] > 0) || !(bk.h[1] > 0) || !(bk.h[2] > 0)) {
+      fail(BSSN_B200_EINVAL, "batch_plan: block " + std::to_string(b) + " has a bad extent, offset or spacing");
+      return -1;
+    }
+    bk.tile0 = (int)t0;
+    t0 += (long long)((bk.sx + tx - 1) / tx) * ((bk.sy + ty - 1) / ty) * ((bk.sz + tz - 1) / tz);
+    if (t0 > (1LL << 30)) {
+      fail(BSSN_B200_EINVAL, "batch_plan: too many tiles");
+      return -1;
+    }
+  }
+  return (int)t0;
 }
 
-int bssn_b200_rhs(void* stream, const double* F, const double* S, double* OUT, long long Sx,
-                  long long Sy, long long Sz, void* scratch, size_t scratch_bytes) {
-  if (!F || !S || !OUT) return fail(BSSN_B200_EINVAL, "rhs: NULL operand");
+int bssn_b200_batch_rhs(void* stream, const double* F, const double* S, double* OUT,
+                        const bssn_b200_block* blocks, int nblocks, int ntiles, int variant) {
+  if (!F || !S || !OUT) return fail(BSSN_B200_EINVAL, "batch_rhs: NULL operand");
+  if (OUT == F) return fail(BSSN_B200_EINVAL, "batch_rhs: OUT must not alias F");
   bssn::Args a{};
   int grid = 0;
-  int rc = prepare(&a, Sx, Sy, Sz, &grid);
-  if (rc) return rc;
-  rc = check_scratch(scratch, scratch_bytes);
+  int rc = prepare_batch(&a, blocks, nblocks, ntiles, variant, &grid);
   if (rc) return rc;
   a.F = F; a.S = S; a.OUT = OUT;
-  a.scratch = static_cast<double*>(scratch);
-  a.use_ko = 0; a.ko_sigma = 0.0;
-  return launch_fused<3, bssn::MODE_RHS>(a, static_cast<cudaStream_t>(stream), grid);
+  return launch_variant<3, bssn::MODE_RHS>(a, static_cast<cudaStream_t>(stream), grid, variant);
 }
 
-int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* Y, double* ACC,
-                        double* YNEXT, const double* S, double ko_sigma, int ko_order,
-                        double chi_floor, double alpha_floor, long long Sx, long long Sy, long long Sz,
-                        void* scratch, size_t scratch_bytes) {
-  if (stage < 0 || stage > 3) return fail(BSSN_B200_EINVAL, "rk4_stage: stage must be 0..3");
-  if (!U || !Y || !ACC || !YNEXT || !S) return fail(BSSN_B200_EINVAL, "rk4_stage: NULL operand");
-  if (YNEXT == Y) return fail(BSSN_B200_EINVAL, "rk4_stage: YNEXT must not alias Y");
-  if (stage < 3 && YNEXT == U) return fail(BSSN_B200_EINVAL, "rk4_stage: YNEXT may alias U only at stage 3");
+int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const double* Y, double* ACC,
+                              double* YNEXT, const double* S, double ko_sigma, int ko_order,
+                              double chi_floor, double alpha_floor, const bssn_b200_block* blocks,
+                              int nblocks, int ntiles, int variant) {
+  if (stage < 0 || stage > 3) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: stage must be 0..3");
+  if (!U || !Y || !ACC || !YNEXT || !S) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: NULL operand");
+  if (YNEXT == Y) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: YNEXT must not alias Y");
+  if (stage < 3 && YNEXT == U) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: YNEXT may alias U only at stage 3");
+  if (ACC == Y || ACC == U || ACC == YNEXT) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: ACC must not alias another operand");
   const bool use_ko = ko_sigma > 0.0;
-  if (use_ko && ko_order != 6 && ko_order != 8) return fail(BSSN_B200_EINVAL, "rk4_stage: ko_order must be 6 or 8");
+  if (use_ko && ko_order != 6 && ko_order != 8) return fail(BSSN_B200_EINVAL, "batch_rk4_stage: ko_order must be 6 or 8");
   bssn::Args a{};
   int grid = 0;
-  int rc = prepare(&a, Sx, Sy, Sz, &grid);
-  if (rc) return rc;
-  rc = check_scratch(scratch, scratch_bytes);
+  int rc = prepare_batch(&a, blocks, nblocks, ntiles, variant, &grid);
   if (rc) return rc;
   a.F = Y; a.U = U; a.ACC = ACC; a.OUT = YNEXT; a.S = S;
-  a.scratch = static_cast<double*>(scratch);
   a.stage = stage;
   a.use_ko = use_ko ? 1 : 0;
   a.ko_sigma = use_ko ? ko_sigma : 0.0;
   a.chi_floor = chi_floor; a.alpha_floor = alpha_floor;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (use_ko && ko_order == 8) return launch_fused<4, bssn::MODE_STAGE>(a, st, grid);
-  return launch_fused<3, bssn::MODE_STAGE>(a, st, grid);
+  if (use_ko && ko_order == 8) return launch_variant<4, bssn::MODE_STAGE>(a, st, grid, variant);
+  return launch_variant<3, bssn::MODE_STAGE>(a, st, grid, variant);
+}
+
+const char* bssn_b200_last_error(void) { return g_err.c_str(); }
+
+const char* bssn_b200_version(void) { return "bssn_b200 0.2 sm_100a"; }
+
+int bssn_b200_rhs(void* stream, const double* F, const double* S, double* OUT, long long Sx,
+                  long long Sy, long long Sz) {
+  if (!F || !S || !OUT) return fail(BSSN_B200_EINVAL, "rhs: NULL operand");
+  if (OUT == F) return fail(BSSN_B200_EINVAL, "rhs: OUT must not alias F");
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  a.F = F; a.S = S; a.OUT = OUT;
+  return launch_stream<3, bssn::MODE_RHS>(a, static_cast<cudaStream_t>(stream), grid);
+}
+
+int bssn_b200_constraints(void* stream, const double* F, const double* S, double* OUT,
+                          long long Sx, long long Sy, long long Sz) {
+  if (!F || !S || !OUT) return fail(BSSN_B200_EINVAL, "constraints: NULL operand");
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  a.F = F; a.S = S; a.OUT = OUT;
+  return launch_stream<3, bssn::MODE_CON>(a, static_cast<cudaStream_t>(stream), grid);
+}
+
+size_t bssn_b200_norms_scratch_bytes(void) {
+  int sms = 0;
+  if (device_sms(&sms)) return 0;
+  return (size_t)sms * 2 * sizeof(double);
+}
+
+int bssn_b200_constraint_norms(void* stream, const double* F, const double* S, long long Sx,
+                               long long Sy, long long Sz, int ng, double* scratch,
+                               size_t scratch_bytes, double* OUT2) {
+  if (!F || !S || !OUT2) return fail(BSSN_B200_EINVAL, "constraint_norms: NULL operand");
+  if (ng < 0 || 2LL * ng >= Sx || 2LL * ng >= Sy || 2LL * ng >= Sz)
+    return fail(BSSN_B200_EINVAL, "constraint_norms: the interior [ng, S-ng) is empty");
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  if (!scratch) return fail(BSSN_B200_EINVAL, "constraint_norms: scratch is NULL");
+  if (scratch_bytes < (size_t)grid * 2 * sizeof(double))
+    return fail(BSSN_B200_EINVAL, "constraint_norms: scratch smaller than bssn_b200_norms_scratch_bytes()");
+  a.F = F; a.S = S; a.ng = ng; a.partials = scratch;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  rc = launch_stream<3, bssn::MODE_NORM>(a, st, grid);
+  if (rc) return rc;
+  const double count = (double)(Sx - 2 * ng) * (double)(Sy - 2 * ng) * (double)(Sz - 2 * ng);
+  bssn::norm_finalize_kernel<<<1, 32, 0, st>>>(scratch, grid, count, OUT2);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail("norm_finalize launch", e);
+  return 0;
+}
+
+int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* Y, double* ACC,
+                        double* YNEXT, const double* S, double ko_sigma, int ko_order,
+                        double chi_floor, double alpha_floor, long long Sx, long long Sy, long long Sz) {
+  if (stage < 0 || stage > 3) return fail(BSSN_B200_EINVAL, "rk4_stage: stage must be 0..3");
+  if (!U || !Y || !ACC || !YNEXT || !S) return fail(BSSN_B200_EINVAL, "rk4_stage: NULL operand");
+  if (YNEXT == Y) return fail(BSSN_B200_EINVAL, "rk4_stage: YNEXT must not alias Y");
+  if (stage < 3 && YNEXT == U) return fail(BSSN_B200_EINVAL, "rk4_stage: YNEXT may alias U only at stage 3");
+  if (ACC == Y || ACC == U || ACC == YNEXT) return fail(BSSN_B200_EINVAL, "rk4_stage: ACC must not alias another operand");
+  const bool use_ko = ko_sigma > 0.0;
+  if (use_ko && ko_order != 6 && ko_order != 8) return fail(BSSN_B200_EINVAL, "rk4_stage: ko_order must be 6 or 8");
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  a.F = Y; a.U = U; a.ACC = ACC; a.OUT = YNEXT; a.S = S;
+  a.stage = stage;
+  a.use_ko = use_ko ? 1 : 0;
+  a.ko_sigma = use_ko ? ko_sigma : 0.0;
+  a.chi_floor = chi_floor; a.alpha_floor = alpha_floor;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (use_ko && ko_order == 8) return launch_stream<4, bssn::MODE_STAGE>(a, st, grid);
+  return launch_stream<3, bssn::MODE_STAGE>(a, st, grid);
 }
 
 int bssn_b200_derivatives(void* stream, const double* F, const double* S, double* DOUT,
@@ -555,26 +922,25 @@ int bssn_b200_derivatives(void* stream, const double* F, const double* S, double
   if (use_ko && ko_order != 6 && ko_order != 8) return fail(BSSN_B200_EINVAL, "derivatives: ko_order must be 6 or 8");
   bssn::Args a{};
   int grid = 0;
-  int rc = prepare(&a, Sx, Sy, Sz, &grid);
+  int rc = prepare(&a, Sx, Sy, Sz, 4, &grid);
   if (rc) return rc;
   a.F = F; a.S = S; a.OUT = DOUT;
-  a.scratch = nullptr;
   a.use_ko = use_ko ? 1 : 0;
   a.ko_sigma = use_ko ? ko_sigma : 0.0;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (use_ko && ko_order == 8) return launch_fused<4, bssn::MODE_DERIV>(a, st, grid);
-  return launch_fused<3, bssn::MODE_DERIV>(a, st, grid);
+  if (use_ko && ko_order == 8) return launch_deriv<4>(a, st, grid);
+  return launch_deriv<3>(a, st, grid);
 }
 
 int bssn_b200_rhs_algebra(void* stream, const double* F, const double* D, const double* S, double* OUT,
                           long long npts) {
   if (!F || !D || !S || !OUT) return fail(BSSN_B200_EINVAL, "rhs_algebra: NULL operand");
   if (npts < 1 || npts > (1LL << 31) - 1) return fail(BSSN_B200_EINVAL, "rhs_algebra: npts out of range");
-  DeviceInfo d;
-  int rc = device_info(&d);
+  int sms = 0;
+  int rc = device_sms(&sms);
   if (rc) return rc;
   long long blocks = (npts + 127) / 128;
-  const long long cap = (long long)d.sms * 16;
+  const long long cap = (long long)sms * 16;
   if (blocks > cap) blocks = cap;
   bssn::algebra_kernel<<<(int)blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(F, D, S, OUT, npts);
   cudaError_t e = cudaGetLastError();
@@ -593,11 +959,11 @@ int bssn_b200_advance_time(void* stream, double* S) {
 int bssn_b200_enforce(void* stream, double* U, long long npts, double chi_floor, double alpha_floor) {
   if (!U) return fail(BSSN_B200_EINVAL, "enforce: NULL operand");
   if (npts < 1) return fail(BSSN_B200_EINVAL, "enforce: npts must be >= 1");
-  DeviceInfo d;
-  int rc = device_info(&d);
+  int sms = 0;
+  int rc = device_sms(&sms);
   if (rc) return rc;
   long long blocks = (npts + 255) / 256;
-  const long long cap = (long long)d.sms * 8;
+  const long long cap = (long long)sms * 8;
   if (blocks > cap) blocks = cap;
   bssn::enforce_kernel<<<(int)blocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(U, npts, chi_floor, alpha_floor);
   cudaError_t e = cudaGetLastError();
@@ -611,12 +977,12 @@ int bssn_b200_periodic_sync(void* stream, double* U, long long Sx, long long Sy,
   if (rc) return rc;
   if (ng < 1 || 3LL * ng > Sx || 3LL * ng > Sy || 3LL * ng > Sz)
     return fail(BSSN_B200_EINVAL, "periodic_sync: need 1 <= ng and 3*ng <= every extent");
-  DeviceInfo d;
-  rc = device_info(&d);
+  int sms = 0;
+  rc = device_sms(&sms);
   if (rc) return rc;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   for (int axis = 0; axis < 3; ++axis) {
-    bssn::periodic_axis_kernel<<<d.sms * 4, 256, 0, st>>>(U, Sx, Sy, Sz, axis, ng);
+    bssn::periodic_axis_kernel<<<sms * 4, 256, 0, st>>>(U, Sx, Sy, Sz, axis, ng);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail("periodic_sync launch", e);
   }

@@ -13,9 +13,10 @@ Fixtures (numpy .npz, float64, exact):
   order, then one per derivative in the reference's sorted derivative-name
   order) and the reference's scalars; outputs from the reference algebra.
 * ``bl_small.npz`` — a Brill-Lindquist state (two punctures, 6^3 interior + 3
-  ghosts on [-4,4]^3), its RHS (restated stencils + reference algebra) and one
+  ghosts on [-4,4]^3), its RHS (restated stencils + reference algebra), one
   RK4 step composed as in 3D/src/bssn3d/evolve.py:125-137 (KO sigma 0.1,
-  order 6, enforcement).
+  order 6, enforcement) and its Hamiltonian/momentum constraints from the
+  reference's compiled physcon block (oracle/_ref/libdendro_physcon.so).
 * ``gauge_wave_rhs.npz`` — the harmonic gauge wave (amplitude 0.01, 8^3
   interior + 3 ghosts on [-1/2,1/2]^3) and its RHS, the data the reference's
   fused-kernel test uses (3D/tests/integration/test_bssn_fused_cuda.py:41-49).
@@ -114,7 +115,10 @@ def main():
     S = pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0), grid.dy, grid.dz)
     rhs = O.ref_rhs(U, S)
     step = rk4_step_reference(U, S, 0.1, 6)
-    np.savez(OUT / "bl_small.npz", U=U, S=S, rhs=rhs, step=step, ko_sigma=0.1, ko_order=6)
+    Dv = O.derivatives(U, grid.dx, grid.dy, grid.dz)
+    H, M = O.ref_constraints_algebra(U, Dv)
+    np.savez(OUT / "bl_small.npz", U=U, S=S, rhs=rhs, step=step, ko_sigma=0.1, ko_order=6,
+             H=H, M=M)
 
     g = Grid.from_domain(8, ng=3)
     W = ID.gauge_wave(g, amplitude=0.01)

@@ -213,21 +213,22 @@ def test_error_paths_do_not_launch():
     lib = L.load()
     F = torch.zeros((24, 8, 8, 8), dtype=torch.float64, device=DEV)
     S = torch.zeros(16, dtype=torch.float64, device=DEV)
-    need = lib.bssn_b200_scratch_bytes(6)
-    assert need > 0
-    scratch = torch.empty(need // 8, dtype=torch.float64, device=DEV)
     out = torch.empty_like(F)
-    rc = lib.bssn_b200_rhs(None, F.data_ptr(), S.data_ptr(), out.data_ptr(), 8, 8, 8, scratch.data_ptr(), 64)
-    assert rc == L.ESCRATCH
-    rc = lib.bssn_b200_rhs(None, F.data_ptr(), S.data_ptr(), out.data_ptr(), 0, 8, 8, scratch.data_ptr(), need)
+    acc = torch.empty_like(F)
+    rc = lib.bssn_b200_rhs(None, F.data_ptr(), S.data_ptr(), out.data_ptr(), 0, 8, 8)
     assert rc == L.EINVAL
-    rc = lib.bssn_b200_rk4_stage(None, 5, F.data_ptr(), F.data_ptr(), out.data_ptr(), out.data_ptr(),
-                                 S.data_ptr(), 0.1, 6, 1e-4, 1e-4, 8, 8, 8, scratch.data_ptr(), need)
+    rc = lib.bssn_b200_rhs(None, F.data_ptr(), S.data_ptr(), F.data_ptr(), 8, 8, 8)
+    assert rc == L.EINVAL                       # OUT aliases F
+    rc = lib.bssn_b200_rk4_stage(None, 5, F.data_ptr(), F.data_ptr(), acc.data_ptr(), out.data_ptr(),
+                                 S.data_ptr(), 0.1, 6, 1e-4, 1e-4, 8, 8, 8)
     assert rc == L.EINVAL
-    rc = lib.bssn_b200_rk4_stage(None, 0, F.data_ptr(), F.data_ptr(), out.data_ptr(), F.data_ptr(),
-                                 S.data_ptr(), 0.1, 6, 1e-4, 1e-4, 8, 8, 8, scratch.data_ptr(), need)
+    rc = lib.bssn_b200_rk4_stage(None, 0, F.data_ptr(), F.data_ptr(), acc.data_ptr(), F.data_ptr(),
+                                 S.data_ptr(), 0.1, 6, 1e-4, 1e-4, 8, 8, 8)
     assert rc == L.EINVAL                       # YNEXT aliases Y
     assert "alias" in lib.bssn_b200_last_error().decode()
+    rc = lib.bssn_b200_rk4_stage(None, 0, F.data_ptr(), F.data_ptr(), acc.data_ptr(), out.data_ptr(),
+                                 S.data_ptr(), 0.1, 7, 1e-4, 1e-4, 8, 8, 8)
+    assert rc == L.EINVAL                       # KO order 7
     torch.cuda.synchronize()
 
 
@@ -237,3 +238,42 @@ def test_nan_input_propagates_without_fault():
     out = _gpu_rhs(F, _S(0.1, 0.1, 0.1))
     assert np.isnan(out).any()
     assert np.isfinite(out[:, 0, 0, 0]).all()
+
+
+# ------------------------------------------------------------ constraints
+def test_constraints_golden_and_norms():
+    from bssn3d_b200.constraints import ConstraintSolver
+    from bssn3d_b200.grid import Grid
+    g = np.load(GOLDEN / "bl_small.npz")
+    grid = Grid.from_domain(6, lo=-4.0, hi=4.0, ng=3)
+    cs = ConstraintSolver(grid)
+    out = cs.constraints_tensor(_dev(g["U"])).cpu().numpy()
+    assert np.abs(out[0] - g["H"]).max() <= 1e-12 * np.abs(g["H"]).max()
+    if np.abs(g["M"]).max() > 0:
+        assert np.abs(out[1:] - g["M"]).max() <= 1e-12 * np.abs(g["M"]).max()
+    h, m = cs.l2(_dev(g["U"]))
+    sl = (slice(3, -3),) * 3
+    assert h == pytest.approx(float(np.sqrt(np.mean(g["H"][sl] ** 2))), rel=1e-12)
+
+
+def test_constraints_random_vs_oracle():
+    from bssn3d_b200.constraints import ConstraintSolver
+    from bssn3d_b200.grid import Grid
+    F = _random_state((19, 21, 23), 8)
+    grid = Grid(Nx=13, Ny=15, Nz=17, dx=0.1, dy=0.11, dz=0.09, ng=3)
+    out = ConstraintSolver(grid).constraints_tensor(_dev(F)).cpu().numpy()
+    H, M = O.constraints(F, 0.1, 0.11, 0.09)
+    assert O.normwise_rel(out, np.concatenate([H[None], M])).max() < 1e-12
+
+
+def test_constraint_norms_fused_vs_oracle_and_reproducible():
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.constraints import ConstraintSolver
+    grid, U, _ = ID.workload(0, n=20)
+    cs = ConstraintSolver(grid)
+    a = cs.l2_tensor(_dev(U)).cpu().numpy()
+    b = cs.l2_tensor(_dev(U)).cpu().numpy()
+    np.testing.assert_array_equal(a, b)                     # fixed-order reduction
+    h, m = O.constraint_norms(U, grid.dx, grid.dy, grid.dz, grid.ng)
+    assert a[0] == pytest.approx(h, rel=1e-12)
+    assert a[1] == pytest.approx(m, rel=1e-12, abs=1e-300)

@@ -143,3 +143,28 @@ def test_periodic_sync():
     np.testing.assert_array_equal(P[:, :3], P[:, 6:9])
     np.testing.assert_array_equal(P[:, -3:], P[:, 3:6])
     np.testing.assert_array_equal(P[:, :, :, :3], P[:, :, :, 6:9])
+
+
+def test_constraints_golden():
+    g = np.load(GOLDEN / "bl_small.npz")
+    S = g["S"]
+    H, M = O.constraints(g["U"], S[13], S[14], S[15])
+    assert np.abs(H - g["H"]).max() <= 1e-13 * np.abs(g["H"]).max()
+    assert np.abs(M - g["M"]).max() <= 1e-13 * max(np.abs(g["M"]).max(), 1e-300) or np.abs(g["M"]).max() == 0
+
+
+def test_constraints_vs_compiled_physcon():
+    if not O.have_physcon():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    rng = np.random.default_rng(21)
+    n = 2048
+    F = 0.1 * rng.uniform(-1, 1, (24, n))
+    F[0] += 1.0
+    F[1] = 0.05 + rng.uniform(0, 1, n)
+    for k in (3, 6, 8):
+        F[k] += 1.0
+    D = 0.5 * rng.standard_normal((138, n))
+    H, M = O.constraints_algebra(F, D)
+    Hr, Mr = O.ref_constraints_algebra(F, D)
+    assert np.abs(H - Hr).max() <= 1e-13 * np.abs(Hr).max()
+    assert np.abs(M - Mr).max() <= 1e-13 * np.abs(Mr).max()
