@@ -146,6 +146,26 @@ int bssn_b200_advance_time(void* stream, double* S);
 int bssn_b200_rhs_algebra(void* stream, const double* F, const double* D,
                           const double* S, double* OUT, long long npts);
 
+/* ---- Ozaki INT8 derivative path (tcgen05 tensor cores) -------------------
+ * The 138 derivatives (+24 KO sums when ko_sigma > 0) of F into DOUT, like
+ * bssn_b200_derivatives, but every stencil is applied as an exact INT8 x INT8
+ * -> INT32 tensor-core contraction of k INT8 digit planes (k = 1..8, one
+ * power-of-two exponent per line along the differentiation axis), recombined
+ * in float64. Mixed second derivatives take the first derivative along the
+ * lower axis through the same path twice. Bit-reproducible run to run.
+ * The reference has no BSSN Ozaki path; its MCS Ozaki derivative
+ * (2D/src/mcs2d/schemes/ozaki.py:257-380) is the design source.
+ * Workspace: caller-provided device memory of bssn_b200_ozaki_workspace_bytes
+ * bytes, 256-byte aligned; a device int at bssn_b200_ozaki_error_flag() is set
+ * to 1 if a tensor-core wait gave up (read it after the stream completes).
+ * Errors: bssn_b200_ozaki_last_error(). */
+size_t bssn_b200_ozaki_workspace_bytes(long long Sx, long long Sy, long long Sz, int k);
+int* bssn_b200_ozaki_error_flag(void* workspace, long long Sx, long long Sy, long long Sz, int k);
+const char* bssn_b200_ozaki_last_error(void);
+int bssn_b200_ozaki_derivatives(void* stream, const double* F, const double* S, double* DOUT, int k,
+                                double ko_sigma, int ko_order, long long Sx, long long Sy,
+                                long long Sz, void* workspace, size_t workspace_bytes);
+
 /* Algebraic enforcement in place (3D/src/bssn3d/evolve.py:93-119). */
 int bssn_b200_enforce(void* stream, double* U, long long npts, double chi_floor,
                       double alpha_floor);

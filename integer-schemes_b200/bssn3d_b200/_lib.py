@@ -37,6 +37,10 @@ _SIGNATURES = {
     "bssn_b200_derivatives": ([_P, _P, _P, _P, _D, _I, _LL, _LL, _LL], _I),
     "bssn_b200_advance_time": ([_P, _P], _I),
     "bssn_b200_rhs_algebra": ([_P, _P, _P, _P, _P, _LL], _I),
+    "bssn_b200_ozaki_workspace_bytes": ([_LL, _LL, _LL, _I], _SZ),
+    "bssn_b200_ozaki_error_flag": ([_P, _LL, _LL, _LL, _I], _P),
+    "bssn_b200_ozaki_last_error": ([], ctypes.c_char_p),
+    "bssn_b200_ozaki_derivatives": ([_P, _P, _P, _P, _I, _D, _I, _LL, _LL, _LL, _P, _SZ], _I),
     "bssn_b200_enforce": ([_P, _P, _LL, _D, _D], _I),
     "bssn_b200_periodic_sync": ([_P, _P, _LL, _LL, _LL, _I], _I),
 }

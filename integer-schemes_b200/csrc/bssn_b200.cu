@@ -76,6 +76,12 @@ struct Weights {
   double wko[3][9];
 };
 
+// Stencil sums are evaluated with separately rounded products and sums, tap
+// by tap from the lowest offset: the same IEEE operations as the reference's
+// `sum(stencil[k] * slice_k)` (derivatives.py:78-88), so the GPU derivatives
+// are bit-identical to it (no FMA contraction).
+__device__ __forceinline__ double tap(double acc, double w, double v) { return __dadd_rn(acc, __dmul_rn(w, v)); }
+
 __device__ __forceinline__ long long clampll(long long v, long long hi) {
   return v < 0 ? 0 : (v > hi ? hi : v);
 }
@@ -119,6 +125,10 @@ struct TileGeom {
   static constexpr int T2N = TX * TY * (TZ + 6);                 // d/dy over the z halo
   static constexpr int T1VOL = TX * T1Y * TP, T2VOL = TX * TY * TP;
   static constexpr size_t SMEM = (2 * (size_t)VOL + T1VOL + T2VOL) * sizeof(double);
+  // + per-point staging of the stage input, u_n and the accumulator (24 each),
+  // when it fits next to the tiles in the 227 KB a CTA may use
+  static constexpr bool PTS = SMEM + (size_t)3 * NFIELD * NTHREADS * sizeof(double) + 1024 <= 232448;
+  static constexpr size_t SMEM_PTS = PTS ? (size_t)3 * NFIELD * NTHREADS * sizeof(double) : 0;
 };
 
 __device__ __forceinline__ Params load_params(const double* __restrict__ S) {
@@ -192,7 +202,7 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
     double acc = 0.0;
 #pragma unroll
     for (int k = 0; k < 7; ++k)
-      if (k != 3) acc += W.w1[a][k] * t[c + (k - 3) * st[a]];
+      if (k != 3) acc = tap(acc, W.w1[a][k], t[c + (k - 3) * st[a]]);
     out[(long long)d1slot(f, a) * n] = acc;
   }
   if (has_d2(f)) {
@@ -200,7 +210,7 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
     for (int a = 0; a < 3; ++a) {
       double acc = 0.0;
 #pragma unroll
-      for (int k = 0; k < 7; ++k) acc += W.w2[a][k] * t[c + (k - 3) * st[a]];
+      for (int k = 0; k < 7; ++k) acc = tap(acc, W.w2[a][k], t[c + (k - 3) * st[a]]);
       out[(long long)d2slot(f, sym(a, a)) * n] = acc;
     }
 #pragma unroll
@@ -214,8 +224,8 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
           double inner = 0.0;
 #pragma unroll
           for (int a = 0; a < 7; ++a)
-            if (a != 3) inner += W.w1[i][a] * t[c + (a - 3) * st[i] + (b - 3) * st[j]];
-          acc += W.w1[j][b] * inner;
+            if (a != 3) inner = tap(inner, W.w1[i][a], t[c + (a - 3) * st[i] + (b - 3) * st[j]]);
+          acc = tap(acc, W.w1[j][b], inner);
         }
         out[(long long)d2slot(f, sym(i, j)) * n] = acc;
       }
@@ -226,8 +236,8 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
     for (int a = 0; a < 3; ++a) {
       double s = 0.0;
 #pragma unroll
-      for (int k = 0; k <= 2 * R; ++k) s += W.wko[a][k] * t[c + (k - R) * st[a]];
-      acc += s;
+      for (int k = 0; k <= 2 * R; ++k) s = tap(s, W.wko[a][k], t[c + (k - R) * st[a]]);
+      acc = __dadd_rn(acc, s);
     }
     out[(long long)(NDERIV + f) * n] = acc;
   }
@@ -277,6 +287,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
   double* const buf1 = smem + Geo::VOL;
   double* const T1 = smem + 2 * Geo::VOL;
   double* const T2 = T1 + Geo::T1VOL;
+  double* const pY = T2 + Geo::T2VOL;      // [24][256] this point's stage-input values
+  double* const pU = pY + NFIELD * NTHREADS;  // [24][256] u_n (stage mode)
+  double* const pA = pU + NFIELD * NTHREADS;  // [24][256] accumulator (stages 1-3)
   __shared__ Weights W;
 
   const int tid = threadIdx.x;
@@ -327,8 +340,28 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
     // points past the array end compute on clamped data and store nothing
     const long long gidx = base + (clampll(gx, Sx - 1) * Sy + clampll(gy, Sy - 1)) * Sz + clampll(gz, Sz - 1);
     const double* __restrict__ Fbase = args.F + base;
+    // Stage this point's 24 values (and, for the RK update, u_n and the
+    // accumulator) in shared memory with one batch of cp.async: each thread
+    // copies and later reads only its own slots, so no barrier is needed.
+    if (Geo::PTS) {
+#pragma unroll
+      for (int k = 0; k < NFIELD; ++k) cp_async8(pY + k * NTHREADS + tid, args.F + gidx + (long long)k * n);
+      cp_async_commit();
+      if (MODE == MODE_STAGE) {
+#pragma unroll
+        for (int k = 0; k < NFIELD; ++k) cp_async8(pU + k * NTHREADS + tid, args.U + gidx + (long long)k * n);
+        if (args.stage > 0) {
+#pragma unroll
+          for (int k = 0; k < NFIELD; ++k) cp_async8(pA + k * NTHREADS + tid, args.ACC + gidx + (long long)k * n);
+        }
+      }
+      cp_async_commit();
+      cp_async_wait<1>();
+    }
     const double* __restrict__ Fp = args.F + gidx;
-    auto fld = [&](int k) -> double { return __ldg(Fp + (long long)k * n); };
+    auto fld = [&](int k) -> double {
+      return Geo::PTS ? pY[k * NTHREADS + tid] : __ldg(Fp + (long long)k * n);
+    };
 
     Stream<RATES, CONS> acc;
     acc.init(fld);
@@ -359,19 +392,19 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
         double s1 = 0.0;
 #pragma unroll
         for (int k = 0; k < 7; ++k)
-          if (k != 3) s1 += W.w1[a][k] * v[k + R - 3];
+          if (k != 3) s1 = tap(s1, W.w1[a][k], v[k + R - 3]);
         d1[a] = s1;
         if (has_d2(f)) {
           double s2 = 0.0;
 #pragma unroll
-          for (int k = 0; k < 7; ++k) s2 += W.w2[a][k] * v[k + R - 3];
+          for (int k = 0; k < 7; ++k) s2 = tap(s2, W.w2[a][k], v[k + R - 3]);
           d2[sym(a, a)] = s2;
         }
         if (use_ko) {
           double sk = 0.0;
 #pragma unroll
-          for (int k = 0; k <= 2 * R; ++k) sk += W.wko[a][k] * v[k];
-          ko += sk;
+          for (int k = 0; k <= 2 * R; ++k) sk = tap(sk, W.wko[a][k], v[k]);
+          ko = __dadd_rn(ko, sk);
         }
       }
       if (has_d2(f)) {
@@ -384,7 +417,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           double s = 0.0;
 #pragma unroll
           for (int k = 0; k < 7; ++k)
-            if (k != 3) s += W.w1[0][k] * cur[cc + (k - 3) * Geo::SX];
+            if (k != 3) s = tap(s, W.w1[0][k], cur[cc + (k - 3) * Geo::SX]);
           T1[(xx * Geo::T1Y + yy) * HZP + zz] = s;
         }
         // T2 = d/dy over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
@@ -396,7 +429,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           double s = 0.0;
 #pragma unroll
           for (int k = 0; k < 7; ++k)
-            if (k != 3) s += W.w1[1][k] * cur[cc + (k - 3) * Geo::SY];
+            if (k != 3) s = tap(s, W.w1[1][k], cur[cc + (k - 3) * Geo::SY]);
           T2[(xx * TY + yy) * HZP + zz] = s;
         }
         __syncthreads();
@@ -406,9 +439,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
 #pragma unroll
         for (int k = 0; k < 7; ++k) {
           if (k == 3) continue;
-          sxy += W.w1[1][k] * T1[t1c + (k - 3) * HZP];
-          sxz += W.w1[2][k] * T1[t1c + (k - 3)];
-          syz += W.w1[2][k] * T2[t2c + (k - 3)];
+          sxy = tap(sxy, W.w1[1][k], T1[t1c + (k - 3) * HZP]);
+          sxz = tap(sxz, W.w1[2][k], T1[t1c + (k - 3)]);
+          syz = tap(syz, W.w1[2][k], T2[t2c + (k - 3)]);
         }
         d2[sym(0, 1)] = sxy;
         d2[sym(0, 2)] = sxz;
@@ -454,14 +487,14 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
       const double dt = P.dt;
       const double hstep = (stage == 2) ? dt : 0.5 * dt;
       const double w6 = dt / 6.0;
-      const double* __restrict__ Up = args.U + gidx;
       double* A = args.ACC + gidx;
       double* O = args.OUT + gidx;
       double en[14];  // stage 3: gt0..5, At0..5, chi, alpha held for enforcement
 #pragma unroll
       for (int q = 0; q < 14; ++q) en[q] = 0.0;
       auto emit = [&](int k, double rate) {
-        const double u = Up[(long long)k * n];
+        const double u = Geo::PTS ? pU[k * NTHREADS + tid] : args.U[gidx + (long long)k * n];
+        const double acc_k = stage == 0 ? 0.0 : (Geo::PTS ? pA[k * NTHREADS + tid] : A[(long long)k * n]);
         if (stage == 0) {
           if (inside) {
             A[(long long)k * n] = rate;
@@ -469,11 +502,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           }
         } else if (stage < 3) {
           if (inside) {
-            A[(long long)k * n] = A[(long long)k * n] + 2.0 * rate;
+            A[(long long)k * n] = acc_k + 2.0 * rate;
             O[(long long)k * n] = u + hstep * rate;
           }
         } else {
-          const double un = u + w6 * (A[(long long)k * n] + rate);
+          const double un = u + w6 * (acc_k + rate);
           if (k >= F_GT && k < F_GT + 6) en[k - F_GT] = un;
           else if (k >= F_AT && k < F_AT + 6) en[6 + k - F_AT] = un;
           else if (k == F_CHI) en[12] = un;
@@ -682,7 +715,7 @@ int set_smem(K kern, size_t smem, int* flags) {
 template <int R, int MODE, class T = bssn::DefaultShape>
 int launch_stream(const bssn::Args& a, cudaStream_t stream, int grid) {
   using Geo = bssn::TileGeom<R, T>;
-  const size_t smem = Geo::SMEM;
+  const size_t smem = Geo::SMEM + Geo::SMEM_PTS;
   auto kern = bssn::stream_kernel<R, MODE, T>;
   static int flags[kMaxDev] = {0};
   int rc = set_smem(kern, smem, flags);

@@ -96,9 +96,11 @@ def test_derivatives_vs_oracle(ko_order, ng):
     S = _S(*h)
     D = derivatives(_dev(F), device_scalars(S, DEV), ko_sigma=0.1, ko_order=ko_order).cpu().numpy()
     ref = O.derivatives(F, *h)
-    assert np.abs(D[:138] - ref).max() <= 1e-11 * np.abs(ref).max()
+    # the reference's bar is 1e-11 absolute; the taps here are the reference's
+    # own IEEE operations in the reference's order, so the bundle is bit-exact
+    np.testing.assert_array_equal(D[:138], ref)
     ko = O.ko(F, *h, 0.1, ko_order)
-    assert np.abs(D[138:] - ko).max() <= 1e-12 * np.abs(ko).max()
+    np.testing.assert_array_equal(D[138:], ko)
 
 
 def test_derivatives_ragged_shape():
@@ -107,7 +109,7 @@ def test_derivatives_ragged_shape():
     h = (0.1, 0.2, 0.05)
     D = derivatives(_dev(F), device_scalars(_S(*h), DEV)).cpu().numpy()
     ref = O.derivatives(F, *h)
-    assert O.normwise_rel(D, ref).max() < 1e-13
+    np.testing.assert_array_equal(D, ref)
 
 
 # -------------------------------------------------------------------- rhs
