@@ -243,5 +243,24 @@ def normwise_rel(a: np.ndarray, b: np.ndarray, floor: float = 1e-300) -> np.ndar
     return np.where(num == 0.0, 0.0, num / den)
 
 
+# tensor groups of the state: alpha, chi, K, gt (6), beta (3), At (6), Gt (3), B (3)
+GROUPS = [[0], [1], [2], list(range(3, 9)), list(range(9, 12)), list(range(12, 18)),
+          list(range(18, 21)), list(range(21, 24))]
+
+
+def normwise_rel_grouped(a: np.ndarray, b: np.ndarray, floor: float = 1e-300) -> np.ndarray:
+    """Per-field max|a-b| divided by the largest |b| over the field's tensor
+    (its 1, 3 or 6 components): a component that is pure seeded noise (an
+    off-diagonal metric entry of 1e-8) is measured against its tensor's size."""
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    num = np.max(np.abs(a - b), axis=1)
+    fmax = np.max(np.abs(b), axis=1)
+    den = np.empty_like(fmax)
+    for g in GROUPS:
+        den[g] = max(float(fmax[g].max()), floor)
+    return np.where(num == 0.0, 0.0, num / den)
+
+
 def set_threads(n: int) -> None:
     os.environ["OMP_NUM_THREADS"] = str(n)

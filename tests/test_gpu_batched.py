@@ -45,13 +45,13 @@ def test_batched_rk4_step_vs_oracle_and_per_block():
     evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=0)
     Ud = torch.from_numpy(U).cuda()
     new = evo.evolve(Ud, dt, 1, t0=0.0).cpu().numpy()
-    for i, b in enumerate(pool.blocks):
-        ref = O.rk4_step(pool.gather(U, i), _S(b.h, dt, 0.0), ko_sigma=0.1, ko_order=6)
-        assert O.normwise_rel(pool.gather(new, i), ref).max() < 1e-12, i
     # one launch per block per stage with the uniform kernel gives the same bytes
     Up = Ud.clone()
     evo.per_block_step_inplace(Up, evo.block_scalars(0.0, dt))
     np.testing.assert_array_equal(Up.cpu().numpy(), new)
+    for i, b in enumerate(pool.blocks):
+        ref = O.rk4_step(pool.gather(U, i), _S(b.h, dt, 0.0), ko_sigma=0.1, ko_order=6)
+        assert O.normwise_rel_grouped(pool.gather(new, i), ref).max() < 1e-12, i
 
 
 def test_batched_variants_agree_and_repeat_bit_identically():
@@ -77,7 +77,7 @@ def test_batched_ko8_ghost4():
     new = evo.evolve(torch.from_numpy(U).cuda(), dt, 1).cpu().numpy()
     for i, b in enumerate(pool.blocks):
         ref = O.rk4_step(pool.gather(U, i), _S(b.h, dt), ko_sigma=0.1, ko_order=8, ng=4)
-        assert O.normwise_rel(pool.gather(new, i), ref).max() < 1e-12
+        assert O.normwise_rel_grouped(pool.gather(new, i), ref).max() < 1e-12
 
 
 def test_autotune_picks_a_variant():

@@ -174,7 +174,7 @@ def test_rk4_step_golden():
     grid = Grid.from_domain(6, lo=-4.0, hi=4.0, ng=3)
     evo = BSSNEvolution(grid, ko_sigma=float(g["ko_sigma"]), bc="none", ko_order=int(g["ko_order"]))
     new = evo.step(BSSNState(_dev(g["U"])), 0.0, float(S[2])).data.cpu().numpy()
-    assert O.normwise_rel(new, g["step"]).max() < 1e-12
+    assert O.normwise_rel_grouped(new, g["step"]).max() < 1e-12
 
 
 @pytest.mark.parametrize("ko_order,ng,bc", [(6, 3, "none"), (8, 4, "none"), (6, 3, "periodic")])
@@ -195,7 +195,7 @@ def test_evolve_vs_oracle(ko_order, ng, bc):
     for s in range(nsteps):
         S[6] = 0.2 + s * dt if s == 0 else S[6] + dt
         ref = O.rk4_step(ref, S, ko_sigma=0.1, ko_order=ko_order, periodic=(bc == "periodic"), ng=ng)
-    assert O.normwise_rel(out, ref).max() < 1e-11
+    assert O.normwise_rel_grouped(out, ref).max() < 1e-12
 
 
 def test_graph_replay_matches_eager():
