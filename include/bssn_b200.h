@@ -111,6 +111,25 @@ int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const do
                               const bssn_b200_block* blocks, int nblocks, int ntiles,
                               int variant);
 
+/* The constraint norms of bssn_b200_constraint_norms for callers that cannot
+ * allocate device memory: an XLA FFI handler (XLA owns every device buffer it
+ * hands over and gives the handler no allocation of its own outside its
+ * scratch protocol), a plugin running inside a host's stream capture (where
+ * cudaMalloc would break the capture), or a loop under a no-allocation rule.
+ * The partial sums live in a file-scope static __device__ array sized for 256
+ * CTAs (4 KB, held on every GPU that loads the library until exit); the
+ * persistent grid uses min(tiles, SMs) CTAs, so any grid fits on GPUs with up
+ * to 256 SMs and a launch that would need more slots is rejected with
+ * BSSN_B200_EINVAL. Inputs and outputs are still the caller's. The first call
+ * on a device resolves the array's device address with cudaGetSymbolAddress,
+ * so make that first call before any stream capture. All calls share the
+ * array (each call overwrites the slots it reads, so nothing needs clearing):
+ * calls that overlap on the GPU — on two streams, or from two host threads —
+ * race. No counterpart in the reference. */
+int bssn_b200_constraint_norms_static(void* stream, const double* F, const double* S,
+                                      long long Sx, long long Sy, long long Sz, int ng,
+                                      double* OUT2);
+
 /* One RK4 stage of BSSNEvolution.step (3D/src/bssn3d/evolve.py:125-137) with
  * the Kreiss-Oliger pass of evolve.py:76-84 and, after stage 3, the
  * enforcement of evolve.py:93-119, fused into the RHS kernel:

@@ -579,6 +579,13 @@ __global__ void norm_finalize_kernel(const double* __restrict__ partials, int np
   }
 }
 
+// Partial-sum slots for bssn_b200_constraint_norms_static, the entry point for
+// callers that cannot allocate device memory. It is a file-scope device array:
+// every GPU that loads this library holds it (4 KB) until the process exits,
+// and every call of that entry point reuses it.
+constexpr int kStaticNormCtas = 256;  // CTAs whose partial sums fit (2 doubles each)
+static __device__ __align__(256) double g_static_norm_partials[2 * kStaticNormCtas];
+
 // t <- t + dt in the device scalar pack, between captured RK4 steps
 // (the fori_loop carry update of 3D/src/bssn3d/evolve.py:186-193).
 __global__ void advance_time_kernel(double* S) {
@@ -922,6 +929,37 @@ int bssn_b200_constraint_norms(void* stream, const double* F, const double* S, l
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail("norm_finalize launch", e);
   return 0;
+}
+
+int bssn_b200_constraint_norms_static(void* stream, const double* F, const double* S, long long Sx,
+                                      long long Sy, long long Sz, int ng, double* OUT2) {
+  if (!F || !S || !OUT2) return fail(BSSN_B200_EINVAL, "constraint_norms_static: NULL operand");
+  if (ng < 0 || 2LL * ng >= Sx || 2LL * ng >= Sy || 2LL * ng >= Sz)
+    return fail(BSSN_B200_EINVAL, "constraint_norms_static: the interior [ng, S-ng) is empty");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return cuda_fail("cudaGetDevice", e);
+  if (dev < 0 || dev >= kMaxDev) return fail(BSSN_B200_EINVAL, "constraint_norms_static: device ordinal out of range");
+  // In host code g_static_norm_partials names a host-side stand-in, not device
+  // memory: resolve its address on this device once, with the device current.
+  static double* addr[kMaxDev] = {nullptr};
+  if (!addr[dev]) {
+    double* p = nullptr;
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), bssn::g_static_norm_partials);
+    if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress(static norm partials)", e);
+    addr[dev] = p;
+  }
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  if (grid > bssn::kStaticNormCtas)
+    return fail(BSSN_B200_EINVAL, "constraint_norms_static: this launch needs " + std::to_string(grid) +
+                                      " CTA partial sums but the static array holds " +
+                                      std::to_string(bssn::kStaticNormCtas) +
+                                      "; use bssn_b200_constraint_norms with a caller buffer");
+  return bssn_b200_constraint_norms(stream, F, S, Sx, Sy, Sz, ng, addr[dev],
+                                    sizeof(double) * 2 * bssn::kStaticNormCtas, OUT2);
 }
 
 int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* Y, double* ACC,
