@@ -43,6 +43,9 @@ UNIT = "Mpoint-updates/s"
 FLOPS_PER_POINT = 6840      # algorithmic FP64 flops per RHS point-update
 KO_FLOPS_PER_POINT = 936    # 24 fields x 3 axes x (7 taps: 7 mul + 6 add)
 STAGE_BYTES = 960           # read Y, U, ACC; write ACC, Y_next (5 x 24 x 8 B)
+# DRAM bytes per point of one stage launch, dram__bytes_read.sum + dram__bytes_write.sum
+# from an ncu capture of the 102^3 case (stage 1), scaled to a launch by its points
+TRAFFIC_BYTES_PER_POINT = 962
 LAST_STAGE_BYTES = 768      # read Y, U, ACC; write U_new
 
 
@@ -343,8 +346,8 @@ def bench_b200(args):
     achieved_tf = flops / (mean_stage * 1e-3) / 1e12
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs"),
                 "unit": "GB/s", "frac": achieved_gbs / peaks.get("hbm_gbs"),
-                "traffic": None, "peak_source": f"{peak_kind} hbm_gbs",
-                "kernel": "bssn::fused_kernel<3,MODE_STAGE> (stages 0-2)",
+                "traffic": TRAFFIC_BYTES_PER_POINT * npts, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "bssn::stream_kernel<3, MODE_STAGE, Shape<4,4,16>> (stages 0-2)",
                 "bytes_per_point": STAGE_BYTES, "points_per_launch": npts,
                 "launch_ms": mean_stage}
     roofline_fp64 = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak,
