@@ -146,6 +146,31 @@ int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* 
                         int ko_order, double chi_floor, double alpha_floor,
                         long long Sx, long long Sy, long long Sz);
 
+/* One stage of the 2-step / 3-stage MSRK step, BSSNEvolution._msrk2_step
+ * (3D/src/bssn3d/evolve.py:139-153), with KO and, after stage 2, enforcement
+ * fused in as for bssn_b200_rk4_stage. coef (HOST, 9 doubles) =
+ * {a20, a21, a30, a31, a32, b0, b1, b2, b3}; node times are t, t + c2*dt,
+ * t + c3*dt with c2 = a20 + a21, c3 = a30 + a31 + a32.
+ *   rate = RHS(Y at the node time) + KO(Y)
+ *   stage 0 (Y = U = y_n, ACC = k0 = f(y_{n-1})):
+ *     OUT = Y2 = U + dt*(a20*k0 + a21*rate)
+ *     OUT2 = U + dt*(a30*k0 + a31*rate)         (partial Y3)
+ *     OUT3 = U + dt*(b0*k0 + b1*rate)           (partial y_{n+1})
+ *     ACC = rate                                (k1: the next step's k0)
+ *   stage 1 (Y = Y2, U = partial Y3, ACC = partial y_{n+1}):
+ *     OUT = Y3 = U + dt*a32*rate;   ACC = ACC + dt*b2*rate
+ *   stage 2 (Y = Y3, U = partial y_{n+1}):
+ *     OUT = y_{n+1} = enforce(U + dt*b3*rate)
+ * S[2] = dt and S[6] = t, the step's start time. Y is read with its stencil
+ * halo, so no output may alias it; the other operands are read only at the
+ * point they are written, so OUT may alias U at stages 1 and 2 and ACC is
+ * updated in place. Stage-0 outputs are distinct from each other and from U. */
+int bssn_b200_msrk_stage(void* stream, int stage, const double* U, const double* Y,
+                         double* ACC, double* OUT, double* OUT2, double* OUT3,
+                         const double* S, const double* coef, double ko_sigma, int ko_order,
+                         double chi_floor, double alpha_floor, long long Sx, long long Sy,
+                         long long Sz);
+
 /* The 138 derivatives of F (and, when ko_sigma > 0, the 24 Kreiss-Oliger sums
  * after them) into DOUT (138 or 162, Sx, Sy, Sz): the derivative bundle of
  * 3D/src/bssn3d/derivative_bundle.py:31-48 / 3D/src/bssn3d/deriv_kernel.py. */

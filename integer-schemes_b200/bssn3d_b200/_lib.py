@@ -35,6 +35,7 @@ _SIGNATURES = {
     "bssn_b200_batch_rhs": ([_P, _P, _P, _P, _P, _I, _I, _I], _I),
     "bssn_b200_batch_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _P, _I, _I, _I], _I),
     "bssn_b200_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _LL, _LL, _LL], _I),
+    "bssn_b200_msrk_stage": ([_P, _I, _P, _P, _P, _P, _P, _P, _P, _P, _D, _I, _D, _D, _LL, _LL, _LL], _I),
     "bssn_b200_derivatives": ([_P, _P, _P, _P, _D, _I, _LL, _LL, _LL], _I),
     "bssn_b200_advance_time": ([_P, _P], _I),
     "bssn_b200_rhs_algebra": ([_P, _P, _P, _P, _P, _LL], _I),

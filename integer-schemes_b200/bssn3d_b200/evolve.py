@@ -7,14 +7,22 @@ enforcement after the last stage) in one kernel. A step is four launches
 (+ a ghost sync per stage for periodic boundaries) and ``evolve`` replays the
 step as a captured CUDA graph. Stage times are t, t+dt/2, t+dt/2, t+dt with
 the full dt in the CAHD factor (evolve.py:121-131).
+
+``integrator="rk4_2_1"`` or ``"rk4_2_2"`` selects the 2-step / 3-stage MSRK
+recurrence instead (evolve.py:139-183; coefficients in ``msrk``): three
+launches of ``bssn_b200_msrk_stage`` per step, each stage folding its rate
+into every later combination it appears in, so no k_i is stored except
+f(y_n), which the next step reuses.
 """
 
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, msrk
 from .fused_rhs import _stream_handle, as_device_state, device_scalars, scalars
 from .grid import Grid
 from .rhs import BSSNSolver
@@ -35,9 +43,11 @@ class BSSNEvolution:
         if bc not in ("periodic", "none"):
             raise ValueError(f"unknown bc {bc!r} (periodic or none)")
         self.bc = bc
-        if integrator != "rk4":
-            raise ValueError(f"integrator {integrator!r} is not provided (rk4 only)")
         self.integrator = integrator
+        self._msrk = None
+        if integrator != "rk4":
+            self._msrk = msrk.get(integrator)
+            self._coef = (ctypes.c_double * 9)(*self._msrk.coef)
         self._bufs = {}
         self._graph = None
 
@@ -73,6 +83,42 @@ class BSSNEvolution:
                                      Sx, Sy, Sz)
         _lib.check(rc)
 
+    def _mstage(self, stage, U, Y, ACC, OUT, OUT2, OUT3, S):
+        lib = _lib.load()
+        _, Sx, Sy, Sz = U.shape
+        src = Y
+        if self.bc == "periodic":
+            Ys = self._buffers(U)["Ys"]
+            Ys.copy_(Y)
+            _lib.check(lib.bssn_b200_periodic_sync(_stream_handle(U.device), Ys.data_ptr(),
+                                                   Sx, Sy, Sz, self.ng))
+            src = Ys
+        p = self.params
+        ptr = lambda t: None if t is None else t.data_ptr()
+        rc = lib.bssn_b200_msrk_stage(_stream_handle(U.device), stage, U.data_ptr(), src.data_ptr(),
+                                      ptr(ACC), OUT.data_ptr(), ptr(OUT2), ptr(OUT3), S.data_ptr(),
+                                      ctypes.cast(self._coef, ctypes.c_void_p), self.ko_sigma,
+                                      self.ko_order, p.chi_floor, p.alpha_floor, Sx, Sy, Sz)
+        _lib.check(rc)
+
+    def _msrk_step_inplace(self, U: torch.Tensor, KP: torch.Tensor, S: torch.Tensor):
+        """One MSRK step in place: U <- y_{n+1}, KP <- f(y_n) (was f(y_{n-1}))."""
+        b = self._buffers(U)
+        Y2, Q3, QF = b["Ya"], b["Yb"], b["ACC"]
+        self._mstage(0, U, U, KP, Y2, Q3, QF, S)
+        self._mstage(1, Q3, Y2, QF, Q3, None, None, S)
+        self._mstage(2, QF, Q3, None, U, None, None, S)
+
+    def _startup_inplace(self, U: torch.Tensor, KP: torch.Tensor, S: torch.Tensor):
+        """The RK4 step that starts an MSRK run, keeping its stage-0 rate
+        f(y_0) (evolve.py:173-175: f0 = rhs(y0), y1 = step(y0))."""
+        b = self._buffers(U)
+        self._stage(0, U, U, b["ACC"], b["Ya"], S)
+        KP.copy_(b["ACC"])
+        self._stage(1, U, b["Ya"], b["ACC"], b["Yb"], S)
+        self._stage(2, U, b["Yb"], b["ACC"], b["Ya"], S)
+        self._stage(3, U, b["Ya"], b["ACC"], U, S)
+
     def _advance_time(self, S: torch.Tensor):
         _lib.check(_lib.load().bssn_b200_advance_time(_stream_handle(S.device), S.data_ptr()))
 
@@ -107,13 +153,41 @@ class BSSNEvolution:
         self._step_inplace(U, self._S(t, dt, U.device))
         return BSSNState(U)
 
+    def msrk_step(self, state: BSSNState, fprev, t: float, dt: float):
+        """One MSRK step (evolve.py:139-153): returns (enforce(y_{n+1}), f(y_n)),
+        the second being the next step's ``fprev``."""
+        if self._msrk is None:
+            raise ValueError("msrk_step needs an rk4_2_* integrator")
+        U = as_device_state(state.data if isinstance(state, BSSNState) else state).clone()
+        KP = as_device_state(fprev.data if isinstance(fprev, BSSNState) else fprev).clone()
+        self._msrk_step_inplace(U, KP, self._S(t, dt, U.device))
+        return BSSNState(U), BSSNState(KP)
+
     def evolve(self, state: BSSNState, dt: float, nsteps: int, t0: float = 0.0,
                use_graph: bool = True) -> BSSNState:
-        """``nsteps`` RK4 steps from t0; the step is captured once as a CUDA graph
-        and replayed, with the time advanced on the device (t <- t + dt)."""
+        """``nsteps`` steps from t0; the step is captured once as a CUDA graph
+        and replayed, with the time advanced on the device (t <- t + dt).
+        An MSRK integrator starts with one RK4 step that also keeps f(y_0),
+        then runs the MSRK recurrence (evolve.py:167-183)."""
         U = as_device_state(state.data if isinstance(state, BSSNState) else state).clone()
         S = self._S(t0, dt, U.device)
         if nsteps <= 0:
+            return BSSNState(U)
+        if self._msrk is not None:
+            KP = torch.empty_like(U)
+            self._startup_inplace(U, KP, S)
+            self._advance_time(S)
+            if nsteps == 1:
+                return BSSNState(U)
+            if not use_graph:
+                for _ in range(int(nsteps) - 1):
+                    self._msrk_step_inplace(U, KP, S)
+                    self._advance_time(S)
+                return BSSNState(U)
+            g, U_g, S_g, K_g = self.capture_msrk(U, S, KP)
+            for _ in range(int(nsteps) - 1):
+                g.replay()
+            U.copy_(U_g)
             return BSSNState(U)
         if not use_graph:
             for _ in range(int(nsteps)):
@@ -147,3 +221,23 @@ class BSSNEvolution:
             self._step_inplace(U_g, S_g)
             self._advance_time(S_g)
         return graph, U_g, S_g
+
+    def capture_msrk(self, U: torch.Tensor, S: torch.Tensor, KP: torch.Tensor):
+        """Capture one MSRK step (3 stages + time advance) on static buffers.
+        Returns (graph, U_static, S_static, KP_static); each replay advances
+        U_static by one step and leaves f(y_n) in KP_static."""
+        U_g, S_g, K_g = U.clone(), S.clone(), KP.clone()
+        self._buffers(U_g)
+        side = torch.cuda.Stream(U_g.device)
+        side.wait_stream(torch.cuda.current_stream(U_g.device))
+        with torch.cuda.stream(side):
+            probe = (U_g.clone(), K_g.clone(), S_g.clone())
+            self._msrk_step_inplace(*probe)
+        torch.cuda.current_stream(U_g.device).wait_stream(side)
+        torch.cuda.synchronize(U_g.device)
+        del probe
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self._msrk_step_inplace(U_g, K_g, S_g)
+            self._advance_time(S_g)
+        return graph, U_g, S_g, K_g

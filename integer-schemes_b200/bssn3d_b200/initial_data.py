@@ -1,8 +1,9 @@
 """Initial data for the BSSN path (host-side input synthesis, numpy float64).
 
-* ``minkowski`` and ``gauge_wave`` restate 3D/src/bssn3d/initial_data.py:28
-  and :72-135 (the harmonic gauge wave used by the reference's fused-kernel
-  test, test_bssn_fused_cuda.py:41-49).
+* ``minkowski``, ``robust_stability`` and ``gauge_wave`` restate
+  3D/src/bssn3d/initial_data.py:28, :58-69 and :72-135 (the harmonic gauge
+  wave is the one the reference's fused-kernel test uses,
+  test_bssn_fused_cuda.py:41-49).
 * ``brill_lindquist`` is new: the reference has no puncture data
   (initial_data.py:1-14). It builds the two-puncture conformally flat data the
   benchmark workloads are quoted on: psi = 1 + m1/(2 r1) + m2/(2 r2) with r
@@ -31,6 +32,16 @@ def minkowski(grid: Grid) -> np.ndarray:
     for k in (ALPHA, CHI, GT0, GT3, GT5):
         data[k] = 1.0
     return data
+
+
+def robust_stability(grid: Grid, amp: float = 1.0e-10, seed: int = 0) -> np.ndarray:
+    """Minkowski plus uniform noise in [-amp, amp) on all 24 fields
+    (initial_data.py:58-69). The noise is drawn with
+    ``numpy.random.default_rng(seed)``, not JAX's PRNG, so the samples differ
+    from the reference's for the same seed; the test it serves (noise must
+    not grow) depends only on the amplitude."""
+    rng = np.random.default_rng(seed)
+    return minkowski(grid) + rng.uniform(-amp, amp, size=(NUM_VARS,) + grid.shape)
 
 
 def gauge_wave(grid: Grid, amplitude: float = 0.01, wavelength: float = None,

@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include <string>
 #include <type_traits>
 
@@ -47,7 +48,7 @@ using DefaultShape = Shape<4, 4, 16>;
 // 16 threads of a half-warp (one or two z rows) hit 16 distinct bank pairs.
 __host__ __device__ constexpr int zpitch(int len) { return len <= 8 ? 8 : ((len - 8 + 15) / 16) * 16 + 8; }
 
-enum Mode : int { MODE_DERIV = 0, MODE_RHS = 1, MODE_STAGE = 2, MODE_CON = 3, MODE_NORM = 4 };
+enum Mode : int { MODE_DERIV = 0, MODE_RHS = 1, MODE_STAGE = 2, MODE_CON = 3, MODE_NORM = 4, MODE_MSRK = 5 };
 
 struct Args {
   const double* F;  // stage input (24, n)
@@ -66,6 +67,10 @@ struct Args {
   const bssn_b200_block* blocks;  // batched mode: block table (device), else NULL
   int nblocks;
   int ntiles;         // batched mode: total tiles over all blocks
+  double* OUT2;       // MSRK stage 0: partial Y3
+  double* OUT3;       // MSRK stage 0: partial y_{n+1}
+  double coef[9];     // MSRK: a20, a21, a30, a31, a32, b0, b1, b2, b3
+  double ctime;       // MSRK: this stage's node (stage time t + ctime * dt)
 };
 
 // Stencil weights, pre-scaled on the device from S like derivatives.py:78-81:
@@ -273,6 +278,45 @@ __global__ void __launch_bounds__(NTHREADS) deriv_kernel(const Args args) {
   }
 }
 
+// Final-stage values of the fields that algebraic enforcement rewrites are
+// held back (gt0..5, At0..5, chi, alpha); the rest are stored directly.
+__device__ __forceinline__ bool hold_for_enforce(double* en, int k, double un) {
+  if (k >= F_GT && k < F_GT + 6) en[k - F_GT] = un;
+  else if (k >= F_AT && k < F_AT + 6) en[6 + k - F_AT] = un;
+  else if (k == F_CHI) en[12] = un;
+  else if (k == F_ALPHA) en[13] = un;
+  else return false;
+  return true;
+}
+
+// Algebraic enforcement of one point (evolve.py:93-119): unit conformal
+// determinant, traceless A~ with the unit-det inverse, chi and alpha floors.
+__device__ __forceinline__ void enforce_point(double* en, double* O, long long n, double chi_floor,
+                                              double alpha_floor) {
+  double* g = en;
+  double* a = en + 6;
+  const double det = g[0] * (g[3] * g[5] - g[4] * g[4]) - g[1] * (g[1] * g[5] - g[4] * g[2]) +
+                     g[2] * (g[1] * g[4] - g[3] * g[2]);
+  const double scale = pow(det, -1.0 / 3.0);
+#pragma unroll
+  for (int q = 0; q < 6; ++q) g[q] = g[q] * scale;
+  const double iuxx = g[3] * g[5] - g[4] * g[4];
+  const double iuxy = g[2] * g[4] - g[1] * g[5];
+  const double iuxz = g[1] * g[4] - g[2] * g[3];
+  const double iuyy = g[0] * g[5] - g[2] * g[2];
+  const double iuyz = g[1] * g[2] - g[0] * g[4];
+  const double iuzz = g[0] * g[3] - g[1] * g[1];
+  const double trA = iuxx * a[0] + iuyy * a[3] + iuzz * a[5] + 2.0 * (iuxy * a[1] + iuxz * a[2] + iuyz * a[4]);
+  const double third = trA / 3.0;
+#pragma unroll
+  for (int q = 0; q < 6; ++q) {
+    O[(long long)(F_GT + q) * n] = g[q];
+    O[(long long)(F_AT + q) * n] = a[q] - g[q] * third;
+  }
+  O[(long long)F_CHI * n] = fmax(en[12], chi_floor);
+  O[(long long)F_ALPHA * n] = fmax(en[13], alpha_floor);
+}
+
 // ---------------------------------------------------------------------------
 // The streaming fused kernel.
 // ---------------------------------------------------------------------------
@@ -333,6 +377,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
       }
     }
     if (MODE == MODE_STAGE) P.t = P0.t + cs * P0.dt;  // stage time t, t+dt/2, t+dt/2, t+dt (evolve.py:125-131)
+    if (MODE == MODE_MSRK) P.t = P0.t + args.ctime * P0.dt;  // node times t, t+c2 dt, t+c3 dt (evolve.py:139-153)
     const int tz = lt % ntz, ty = (lt / ntz) % nty, tx = lt / (ntz * nty);
     const long long x0 = (long long)tx * TX, y0 = (long long)ty * TY, z0 = (long long)tz * TZ;
     const long long gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
@@ -347,10 +392,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
 #pragma unroll
       for (int k = 0; k < NFIELD; ++k) cp_async8(pY + k * NTHREADS + tid, args.F + gidx + (long long)k * n);
       cp_async_commit();
-      if (MODE == MODE_STAGE) {
+      if (MODE == MODE_STAGE || MODE == MODE_MSRK) {
 #pragma unroll
         for (int k = 0; k < NFIELD; ++k) cp_async8(pU + k * NTHREADS + tid, args.U + gidx + (long long)k * n);
-        if (args.stage > 0) {
+        if (MODE == MODE_STAGE ? args.stage > 0 : args.stage < 2) {
 #pragma unroll
           for (int k = 0; k < NFIELD; ++k) cp_async8(pA + k * NTHREADS + tid, args.ACC + gidx + (long long)k * n);
         }
@@ -482,7 +527,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
         }
       };
       acc.finalize(fld, P, [](int, double) {}, con);
-    } else {
+    } else if (MODE == MODE_STAGE) {
       const int stage = args.stage;
       const double dt = P.dt;
       const double hstep = (stage == 2) ? dt : 0.5 * dt;
@@ -507,39 +552,46 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           }
         } else {
           const double un = u + w6 * (acc_k + rate);
-          if (k >= F_GT && k < F_GT + 6) en[k - F_GT] = un;
-          else if (k >= F_AT && k < F_AT + 6) en[6 + k - F_AT] = un;
-          else if (k == F_CHI) en[12] = un;
-          else if (k == F_ALPHA) en[13] = un;
-          else if (inside) O[(long long)k * n] = un;
+          if (!hold_for_enforce(en, k, un) && inside) O[(long long)k * n] = un;
         }
       };
       acc.finalize(fld, P, emit, NoCon());
-      if (stage == 3 && inside) {
-        // algebraic enforcement, evolve.py:93-119
-        double* g = en;
-        double* a = en + 6;
-        const double det = g[0] * (g[3] * g[5] - g[4] * g[4]) - g[1] * (g[1] * g[5] - g[4] * g[2]) +
-                           g[2] * (g[1] * g[4] - g[3] * g[2]);
-        const double scale = pow(det, -1.0 / 3.0);
+      if (stage == 3 && inside) enforce_point(en, O, n, args.chi_floor, args.alpha_floor);
+    } else {
+      // 2-step / 3-stage MSRK (evolve.py:139-153). Stage 0 evaluates k1 = f(y_n)
+      // (U = y_n, ACC = k0 = f(y_{n-1}) in, k1 out), stage 1 k2 at Y2 (U = partial
+      // Y3, ACC = partial y_{n+1}), stage 2 k3 at Y3 (U = partial y_{n+1}).
+      const int stage = args.stage;
+      const double dt = P.dt;
+      const double* c = args.coef;
+      double* A = args.ACC + gidx;
+      double* O = args.OUT + gidx;
+      double en[14];
 #pragma unroll
-        for (int q = 0; q < 6; ++q) g[q] = g[q] * scale;
-        const double iuxx = g[3] * g[5] - g[4] * g[4];
-        const double iuxy = g[2] * g[4] - g[1] * g[5];
-        const double iuxz = g[1] * g[4] - g[2] * g[3];
-        const double iuyy = g[0] * g[5] - g[2] * g[2];
-        const double iuyz = g[1] * g[2] - g[0] * g[4];
-        const double iuzz = g[0] * g[3] - g[1] * g[1];
-        const double trA = iuxx * a[0] + iuyy * a[3] + iuzz * a[5] + 2.0 * (iuxy * a[1] + iuxz * a[2] + iuyz * a[4]);
-        const double third = trA / 3.0;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          O[(long long)(F_GT + q) * n] = g[q];
-          O[(long long)(F_AT + q) * n] = a[q] - g[q] * third;
+      for (int q = 0; q < 14; ++q) en[q] = 0.0;
+      auto emit = [&](int k, double rate) {
+        const long long o = (long long)k * n;
+        const double u = Geo::PTS ? pU[k * NTHREADS + tid] : args.U[gidx + o];
+        const double a = stage == 2 ? 0.0 : (Geo::PTS ? pA[k * NTHREADS + tid] : A[o]);
+        if (stage == 0) {
+          if (inside) {
+            A[o] = rate;
+            O[o] = u + dt * (c[0] * a + c[1] * rate);
+            args.OUT2[gidx + o] = u + dt * (c[2] * a + c[3] * rate);
+            args.OUT3[gidx + o] = u + dt * (c[5] * a + c[6] * rate);
+          }
+        } else if (stage == 1) {
+          if (inside) {
+            O[o] = u + dt * (c[4] * rate);
+            A[o] = a + dt * (c[7] * rate);
+          }
+        } else {
+          const double un = u + dt * (c[8] * rate);
+          if (!hold_for_enforce(en, k, un) && inside) O[o] = un;
         }
-        O[(long long)F_CHI * n] = fmax(en[12], args.chi_floor);
-        O[(long long)F_ALPHA * n] = fmax(en[13], args.alpha_floor);
-      }
+      };
+      acc.finalize(fld, P, emit, NoCon());
+      if (stage == 2 && inside) enforce_point(en, O, n, args.chi_floor, args.alpha_floor);
     }
   }
   if (MODE == MODE_NORM) {
@@ -984,6 +1036,47 @@ int bssn_b200_rk4_stage(void* stream, int stage, const double* U, const double* 
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (use_ko && ko_order == 8) return launch_stream<4, bssn::MODE_STAGE>(a, st, grid);
   return launch_stream<3, bssn::MODE_STAGE>(a, st, grid);
+}
+
+int bssn_b200_msrk_stage(void* stream, int stage, const double* U, const double* Y, double* ACC,
+                         double* OUT, double* OUT2, double* OUT3, const double* S, const double* coef,
+                         double ko_sigma, int ko_order, double chi_floor, double alpha_floor,
+                         long long Sx, long long Sy, long long Sz) {
+  if (stage < 0 || stage > 2) return fail(BSSN_B200_EINVAL, "msrk_stage: stage must be 0..2");
+  if (!U || !Y || !OUT || !S || !coef) return fail(BSSN_B200_EINVAL, "msrk_stage: NULL operand");
+  if (stage < 2 && !ACC) return fail(BSSN_B200_EINVAL, "msrk_stage: ACC is required at stages 0 and 1");
+  if (stage == 0 && (!OUT2 || !OUT3)) return fail(BSSN_B200_EINVAL, "msrk_stage: OUT2 and OUT3 are required at stage 0");
+  for (int i = 0; i < 9; ++i)
+    if (!std::isfinite(coef[i])) return fail(BSSN_B200_EINVAL, "msrk_stage: coefficients must be finite");
+  // Y is read with its stencil halo: no output may overwrite it
+  if (OUT == Y || (stage < 2 && ACC == Y) || (stage == 0 && (OUT2 == Y || OUT3 == Y)))
+    return fail(BSSN_B200_EINVAL, "msrk_stage: an output aliases the stage input Y");
+  if (stage == 0) {
+    const void* outs[4] = {ACC, OUT, OUT2, OUT3};
+    for (int i = 0; i < 4; ++i) {
+      if (outs[i] == U) return fail(BSSN_B200_EINVAL, "msrk_stage: stage-0 outputs must not alias U");
+      for (int j = i + 1; j < 4; ++j)
+        if (outs[i] == outs[j]) return fail(BSSN_B200_EINVAL, "msrk_stage: stage-0 outputs must be distinct");
+    }
+  } else if (stage == 1 && (ACC == U || ACC == OUT)) {
+    return fail(BSSN_B200_EINVAL, "msrk_stage: ACC must not alias U or OUT at stage 1");
+  }
+  const bool use_ko = ko_sigma > 0.0;
+  if (use_ko && ko_order != 6 && ko_order != 8) return fail(BSSN_B200_EINVAL, "msrk_stage: ko_order must be 6 or 8");
+  bssn::Args a{};
+  int grid = 0;
+  int rc = prepare(&a, Sx, Sy, Sz, 1, &grid);
+  if (rc) return rc;
+  a.F = Y; a.U = U; a.ACC = ACC; a.OUT = OUT; a.OUT2 = OUT2; a.OUT3 = OUT3; a.S = S;
+  for (int i = 0; i < 9; ++i) a.coef[i] = coef[i];
+  a.ctime = stage == 0 ? 0.0 : (stage == 1 ? coef[0] + coef[1] : coef[2] + coef[3] + coef[4]);
+  a.stage = stage;
+  a.use_ko = use_ko ? 1 : 0;
+  a.ko_sigma = use_ko ? ko_sigma : 0.0;
+  a.chi_floor = chi_floor; a.alpha_floor = alpha_floor;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (use_ko && ko_order == 8) return launch_stream<4, bssn::MODE_MSRK>(a, st, grid);
+  return launch_stream<3, bssn::MODE_MSRK>(a, st, grid);
 }
 
 int bssn_b200_derivatives(void* stream, const double* F, const double* S, double* DOUT,

@@ -591,3 +591,53 @@ void oracle_rk4_step(const double* U, long Sx, long Sy, long Sz, const double* S
   free(Y);
   free(work);
 }
+
+/* rate = RHS + KO at the stage time S[6] (the evaluation BSSNEvolution.rhs
+ * makes, evolve.py:86-91). */
+void oracle_rate(const double* U, long Sx, long Sy, long Sz, const double* S,
+                 double ko_sigma, int ko_order, int periodic, int ng, double* rate) {
+  double* work = (double*)malloc(sizeof(double) * NF * Sx * Sy * Sz);
+  stage_rate(U, Sx, Sy, Sz, S, ko_sigma, ko_order, periodic, ng, rate, work);
+  free(work);
+}
+
+/* One 2-step / 3-stage MSRK step of BSSNEvolution._msrk2_step
+ * (evolve.py:139-153) + enforce. coef = {a20, a21, a30, a31, a32, b0, b1, b2, b3}.
+ * Kprev = f(y_{n-1}) (stage 0 of the method, reused); K_out receives
+ * k1 = f(y_n), the next step's Kprev. Nodes c2 = a20 + a21 and
+ * c3 = a30 + a31 + a32 give the stage times; dt is the full step throughout. */
+void oracle_msrk2_step(const double* U, const double* Kprev, long Sx, long Sy, long Sz,
+                       const double* S_in, const double* coef, double ko_sigma, int ko_order,
+                       int periodic, int ng, double chi_floor, double alpha_floor,
+                       double* U_out, double* K_out) {
+  const long n = Sx * Sy * Sz;
+  const long N = NF * n;
+  double S[16];
+  memcpy(S, S_in, sizeof(S));
+  const double dt = S[2], t = S[6];
+  const double a20 = coef[0], a21 = coef[1], a30 = coef[2], a31 = coef[3], a32 = coef[4];
+  const double* b = coef + 5;
+  double* k1 = (double*)malloc(sizeof(double) * N);
+  double* k2 = (double*)malloc(sizeof(double) * N);
+  double* k3 = (double*)malloc(sizeof(double) * N);
+  double* Y = (double*)malloc(sizeof(double) * N);
+  double* work = (double*)malloc(sizeof(double) * N);
+  const double* k0 = Kprev;
+  S[6] = t;
+  stage_rate(U, Sx, Sy, Sz, S, ko_sigma, ko_order, periodic, ng, k1, work);
+  for (long q = 0; q < N; ++q) Y[q] = U[q] + dt * (a20 * k0[q] + a21 * k1[q]);
+  S[6] = t + (a20 + a21) * dt;
+  stage_rate(Y, Sx, Sy, Sz, S, ko_sigma, ko_order, periodic, ng, k2, work);
+  for (long q = 0; q < N; ++q) Y[q] = U[q] + dt * (a30 * k0[q] + a31 * k1[q] + a32 * k2[q]);
+  S[6] = t + (a30 + a31 + a32) * dt;
+  stage_rate(Y, Sx, Sy, Sz, S, ko_sigma, ko_order, periodic, ng, k3, work);
+  for (long q = 0; q < N; ++q)
+    U_out[q] = U[q] + dt * (b[0] * k0[q] + b[1] * k1[q] + b[2] * k2[q] + b[3] * k3[q]);
+  oracle_enforce(U_out, n, chi_floor, alpha_floor);
+  memcpy(K_out, k1, sizeof(double) * N);
+  free(k1);
+  free(k2);
+  free(k3);
+  free(Y);
+  free(work);
+}

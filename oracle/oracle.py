@@ -60,6 +60,8 @@ def lib():
         L.oracle_constraints_algebra.argtypes = [_L, _P, _P, _P, _P]
         L.oracle_periodic_sync.argtypes = [_P, _L, _L, _L, _I]
         L.oracle_rk4_step.argtypes = [_P, _L, _L, _L, _P, _D, _I, _I, _I, _D, _D, _P]
+        L.oracle_rate.argtypes = [_P, _L, _L, _L, _P, _D, _I, _I, _I, _P]
+        L.oracle_msrk2_step.argtypes = [_P, _P, _L, _L, _L, _P, _P, _D, _I, _I, _I, _D, _D, _P, _P]
         _lib = L
     return _lib
 
@@ -232,6 +234,46 @@ def rk4_step(F: np.ndarray, S: np.ndarray, ko_sigma=0.1, ko_order=6,
     lib().oracle_rk4_step(_ptr(F), Sx, Sy, Sz, _ptr(S), ko_sigma, ko_order,
                           int(periodic), ng, chi_floor, alpha_floor, _ptr(out))
     return out
+
+
+def rate(F: np.ndarray, S: np.ndarray, ko_sigma=0.1, ko_order=6, periodic=False, ng=3) -> np.ndarray:
+    """RHS + KO at time S[6] (BSSNEvolution.rhs, evolve.py:86-91)."""
+    F = _c(F)
+    S = _c(S)
+    _, Sx, Sy, Sz = F.shape
+    out = np.empty_like(F)
+    lib().oracle_rate(_ptr(F), Sx, Sy, Sz, _ptr(S), ko_sigma, ko_order, int(periodic), ng, _ptr(out))
+    return out
+
+
+def msrk2_step(F: np.ndarray, fprev: np.ndarray, S: np.ndarray, coef, ko_sigma=0.1, ko_order=6,
+               periodic=False, ng=3, chi_floor=1e-4, alpha_floor=1e-4):
+    """One 2-step / 3-stage MSRK step + enforce (evolve.py:139-153).
+    coef = (a20, a21, a30, a31, a32, b0, b1, b2, b3). Returns (y_{n+1}, f(y_n))."""
+    F = _c(F)
+    K = _c(fprev)
+    S = _c(S)
+    c = _c(np.asarray(coef, dtype=np.float64))
+    _, Sx, Sy, Sz = F.shape
+    out = np.empty_like(F)
+    kout = np.empty_like(F)
+    lib().oracle_msrk2_step(_ptr(F), _ptr(K), Sx, Sy, Sz, _ptr(S), _ptr(c), ko_sigma, ko_order,
+                            int(periodic), ng, chi_floor, alpha_floor, _ptr(out), _ptr(kout))
+    return out, kout
+
+
+def msrk_evolve(F: np.ndarray, S: np.ndarray, coef, nsteps: int, ko_sigma=0.1, ko_order=6,
+                periodic=False, ng=3) -> np.ndarray:
+    """BSSNEvolution.evolve with an MSRK integrator (evolve.py:167-183):
+    f0 = rate(y0), one RK4 step, then nsteps-1 MSRK steps. S[6] is t0."""
+    S = _c(S).copy()
+    dt = S[2]
+    f = rate(F, S, ko_sigma, ko_order, periodic, ng)
+    y = rk4_step(F, S, ko_sigma, ko_order, periodic, ng)
+    for _ in range(1, int(nsteps)):
+        S[6] = S[6] + dt
+        y, f = msrk2_step(y, f, S, coef, ko_sigma, ko_order, periodic, ng)
+    return y
 
 
 def normwise_rel(a: np.ndarray, b: np.ndarray, floor: float = 1e-300) -> np.ndarray:
