@@ -41,7 +41,37 @@ typedef struct bssn_b200_block {
   int sx, sy, sz;   /* padded extents (ghosts included) */
   int tile0;        /* first tile of the block, filled by bssn_b200_batch_plan */
   double h[3];      /* grid spacing dx, dy, dz */
+  int core;         /* ghost layers the batched kernels leave alone: tiles cover
+                       [core, s - core) on each axis (0 = the whole array; set it
+                       to the ghost width when bssn_b200_fill supplies the ghosts) */
+  int reserved;     /* 0 */
 } bssn_b200_block;
+
+/* One box of a ghost-fill plan (bssn_b200_fill). Every destination point
+ * d = (x, y, z) of the half-open box [lo, hi) in block `dst` (local indices
+ * of its padded array) receives all 24 fields from block `src`:
+ *   BSSN_B200_FILL_COPY      src[d + shift]          same-level copy
+ *   BSSN_B200_FILL_RESTRICT  src[2 d + shift]        fine-to-coarse injection
+ *   BSSN_B200_FILL_PROLONG   node-centred 2:1 prolongation from the coarser
+ *       block src: per axis g = d + shift is the point's index on the refined
+ *       src lattice; even g copies src node g/2, odd g takes the 6-point
+ *       midpoint Lagrange stencil on src nodes (g-1)/2 - 2 ... (g-1)/2 + 3,
+ *       indices clamped to the src array (its edge padding); applied x, then
+ *       y, then z like the reference's sequential passes
+ *       (3D/src/multipatch/amr/kernels.py:52-71,76-102).
+ * Offsets and shapes are those of the block pool (bssn_b200_block). */
+#define BSSN_B200_FILL_COPY 0
+#define BSSN_B200_FILL_RESTRICT 1
+#define BSSN_B200_FILL_PROLONG 2
+
+typedef struct bssn_b200_fill_op {
+  long long dst_off, src_off; /* first double of each block in the pool */
+  long long point0;           /* first point of the box in the launch, set by bssn_b200_fill_plan */
+  int dst_s[3], src_s[3];     /* padded extents of the two blocks */
+  int lo[3], hi[3];           /* destination box, half-open, dst-local */
+  int shift[3];               /* index map (see above) */
+  int kind;                   /* BSSN_B200_FILL_* */
+} bssn_b200_fill_op;
 
 /* Tile-shape variants of the batched kernels (the autotuner's search space):
  * 0 = 4x4x16, 1 = 2x8x16, 2 = 4x8x8, 3 = 8x4x8 points (x, y, z). */
@@ -110,6 +140,26 @@ int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const do
                               int ko_order, double chi_floor, double alpha_floor,
                               const bssn_b200_block* blocks, int nblocks, int ntiles,
                               int variant);
+
+/* Validates a ghost-fill plan held in HOST memory against a pool of
+ * `pool_doubles` doubles (every box inside its destination array, every
+ * copied or injected source point inside its source array, no block past the
+ * pool's end), fills each op's point0 with the prefix of box volumes and
+ * returns the total point count, or -1 (with bssn_b200_last_error). Upload
+ * the filled table for bssn_b200_fill. */
+long long bssn_b200_fill_plan(bssn_b200_fill_op* host_ops, int nops, long long pool_doubles);
+
+/* Executes one planned list of fill boxes on `pool` (one launch, one thread
+ * per destination point, 24 fields each). `ops` is the table in DEVICE
+ * memory, `npoints` the value bssn_b200_fill_plan returned for it, `wmid`
+ * (HOST, 6 doubles) the midpoint Lagrange weights for offsets -2..3 at +1/2.
+ * The boxes of one list must be disjoint and must not write what another box
+ * of the list reads: a same-level list writes ghosts and reads interiors,
+ * and a prolongation list reads a coarser level that is complete before it
+ * runs. No 3D/src/bssn3d counterpart (the reference has no BSSN AMR); the
+ * operators are those of 3D/src/multipatch/amr/kernels.py and sync.py. */
+int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int nops,
+                   long long npoints, const double* wmid);
 
 /* The constraint norms of bssn_b200_constraint_norms for callers that cannot
  * allocate device memory: an XLA FFI handler (XLA owns every device buffer it

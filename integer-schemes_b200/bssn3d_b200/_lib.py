@@ -32,6 +32,8 @@ _SIGNATURES = {
     "bssn_b200_constraint_norms": ([_P, _P, _P, _LL, _LL, _LL, _I, _P, _SZ, _P], _I),
     "bssn_b200_constraint_norms_static": ([_P, _P, _P, _LL, _LL, _LL, _I, _P], _I),
     "bssn_b200_batch_plan": ([_P, _I, _I], _I),
+    "bssn_b200_fill_plan": ([_P, _I, _LL], _LL),
+    "bssn_b200_fill": ([_P, _P, _P, _I, _LL, _P], _I),
     "bssn_b200_batch_rhs": ([_P, _P, _P, _P, _P, _I, _I, _I], _I),
     "bssn_b200_batch_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _P, _I, _I, _I], _I),
     "bssn_b200_rk4_stage": ([_P, _I, _P, _P, _P, _P, _P, _D, _I, _D, _D, _LL, _LL, _LL], _I),

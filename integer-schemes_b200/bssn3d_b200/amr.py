@@ -9,9 +9,16 @@ ghost zones filled from the analytic Brill-Lindquist formula, stored back to
 back in one pooled device buffer, plus the block table the batched kernels
 walk (one persistent launch per RK stage over every block).
 
-Blocks are evolved independently: each block's ghosts are part of its array
-and are updated by the same clamped-stencil RHS as on a single uniform block
-(inter-block ghost exchange and prolongation are the next step, not built).
+Ghosts, two ways (``BatchedEvolution(ghosts=...)``):
+
+* ``"evolve"``: each block is evolved on its own, ghosts included, with the
+  same clamped-stencil RHS as a single uniform block;
+* ``"exchange"``: before every stage the ghosts are refilled from the other
+  blocks (same-level copies, prolongation from the level below; the plan is
+  built in :mod:`bssn3d_b200.ghosts`), and the stage kernels update the
+  interiors only, like the reference's AMR step
+  (3D/src/multipatch/amr/evolve.py:94-147). Ghosts with no source block keep
+  their initial values (a frozen outer boundary).
 
 Pool layout: block b occupies doubles [offset_b, offset_b + 24*n_b) with
 n_b = Sx*Sy*Sz, field f of block b at offset_b + f*n_b, each field C order
@@ -35,7 +42,8 @@ class BlockDesc(ctypes.Structure):
     _fields_ = [("offset", ctypes.c_longlong),
                 ("sx", ctypes.c_int), ("sy", ctypes.c_int), ("sz", ctypes.c_int),
                 ("tile0", ctypes.c_int),
-                ("h", ctypes.c_double * 3)]
+                ("h", ctypes.c_double * 3),
+                ("core", ctypes.c_int), ("reserved", ctypes.c_int)]
 
 
 @dataclass(frozen=True)
@@ -130,7 +138,9 @@ class BlockPool:
         self.tile = tuple(tile)
         self.table, self.ntiles = self.descriptors(self.tile)
 
-    def descriptors(self, tile):
+    def descriptors(self, tile, core: bool = False):
+        """Block table and tile count; ``core=True`` leaves each block's ghost
+        layers out of the tiles (they come from a ghost fill)."""
         TX, TY, TZ = tile
         arr = (BlockDesc * len(self.blocks))()
         t0 = 0
@@ -141,7 +151,9 @@ class BlockPool:
             d.sx, d.sy, d.sz = sx, sy, sz
             d.tile0 = t0
             d.h[0] = d.h[1] = d.h[2] = b.h
-            t0 += -(-sx // TX) * -(-sy // TY) * -(-sz // TZ)
+            d.core = b.ng if core else 0
+            c2 = 2 * d.core
+            t0 += -(-(sx - c2) // TX) * -(-(sy - c2) // TY) * -(-(sz - c2) // TZ)
         return arr, t0
 
     @property
@@ -184,10 +196,15 @@ class BatchedEvolution:
     """
 
     def __init__(self, pool: BlockPool, params=None, ko_sigma: float = 0.1, ko_order: int = 6,
-                 variant: int = 0, device="cuda"):
+                 variant: int = 0, device="cuda", ghosts: str = "evolve", restrict: bool = False):
         import torch
         from .state import PhysicsParams
         from . import _lib
+        if ghosts not in ("evolve", "exchange"):
+            raise ValueError(f"ghosts must be 'evolve' or 'exchange', not {ghosts!r}")
+        if restrict and ghosts != "exchange":
+            raise ValueError("restrict needs ghosts='exchange'")
+        self.ghosts = ghosts
         self.pool = pool
         self.params = params or PhysicsParams()
         self.ko_sigma = float(ko_sigma)
@@ -197,13 +214,19 @@ class BatchedEvolution:
             raise ValueError(f"KO order {ko_order} needs ng >= {ng_need} on every block")
         self.device = torch.device(device)
         self._lib = _lib
+        self.plan = None
+        self.dplan = None
+        if ghosts == "exchange":
+            from .ghosts import DevicePlan, GhostPlan
+            self.plan = GhostPlan(pool, restrict=restrict)
+            self.dplan = DevicePlan(self.plan, self.device)
         self.set_variant(variant)
         self._bufs = None
 
     def set_variant(self, variant: int) -> None:
         import torch
         lib = self._lib.load()
-        table, _ = self.pool.descriptors(self.pool.tile)
+        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange")
         ntiles = lib.bssn_b200_batch_plan(ctypes.addressof(table), len(self.pool.blocks), int(variant))
         if ntiles < 0:
             self._lib.check(self._lib.EINVAL)
@@ -225,7 +248,27 @@ class BatchedEvolution:
         import torch
         if self._bufs is None or self._bufs["Ya"].shape != U.shape:
             self._bufs = {k: torch.empty_like(U) for k in ("Ya", "Yb", "ACC")}
+            if self.ghosts == "exchange":
+                self.seed_buffers(U)
         return self._bufs
+
+    def seed_buffers(self, U):
+        """With ghost exchange the stage kernels write interiors only, so the
+        stage buffers' unfilled ghosts (the frozen outer boundary) must hold
+        U's values: copy U into them."""
+        b = self.buffers(U)
+        b["Ya"].copy_(U)
+        b["Yb"].copy_(U)
+
+    def fill(self, Y):
+        """Refill the ghosts of the pooled state Y, coarse level first."""
+        if self.dplan is not None:
+            self.dplan.run("fill", Y, self._stream())
+
+    def restrict(self, U):
+        """Inject fine interiors into the coarser levels, finest first."""
+        if self.dplan is not None:
+            self.dplan.run("restrict", U, self._stream())
 
     def stage(self, stage, U, Y, ACC, YNEXT, S):
         p = self.params
@@ -237,9 +280,16 @@ class BatchedEvolution:
         self._lib.check(rc)
 
     def rhs(self, U, S):
-        """Pooled RHS (no KO), the batched ``cuda_fused_algebra``."""
+        """Pooled RHS (no KO), the batched ``cuda_fused_algebra``. With ghost
+        exchange the ghosts of a copy of U are filled first and only the
+        interiors of the result are written (the rest is zero)."""
         import torch
-        out = torch.empty_like(U)
+        if self.ghosts == "exchange":
+            U = U.clone()
+            self.fill(U)
+            out = torch.zeros_like(U)
+        else:
+            out = torch.empty_like(U)
         rc = self._lib.load().bssn_b200_batch_rhs(self._stream(), U.data_ptr(), S.data_ptr(), out.data_ptr(),
                                                   self.table_dev.data_ptr(), len(self.pool.blocks),
                                                   self.ntiles, self.variant)
@@ -248,10 +298,12 @@ class BatchedEvolution:
 
     def step_inplace(self, U, S):
         b = self.buffers(U)
-        self.stage(0, U, U, b["ACC"], b["Ya"], S)
-        self.stage(1, U, b["Ya"], b["ACC"], b["Yb"], S)
-        self.stage(2, U, b["Yb"], b["ACC"], b["Ya"], S)
-        self.stage(3, U, b["Ya"], b["ACC"], U, S)
+        for stage, (y, ynext) in enumerate([(U, b["Ya"]), (b["Ya"], b["Yb"]), (b["Yb"], b["Ya"]),
+                                            (b["Ya"], U)]):
+            self.fill(y)
+            self.stage(stage, U, y, b["ACC"], ynext, S)
+        if self.plan is not None and self.plan.restrict_lists:
+            self.restrict(U)
 
     def advance_time(self, S):
         self._lib.check(self._lib.load().bssn_b200_advance_time(self._stream(), S.data_ptr()))
@@ -262,6 +314,8 @@ class BatchedEvolution:
         import torch
         U_g, S_g = U.clone(), S.clone()
         self.buffers(U_g)
+        if self.ghosts == "exchange":
+            self.seed_buffers(U_g)
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
@@ -286,7 +340,10 @@ class BatchedEvolution:
     # -- the comparison point: one launch per block per stage ----------------
     def per_block_step_inplace(self, U, S_blocks):
         """The same RK4 step with one uniform-kernel launch per block per
-        stage (``S_blocks[i]`` carries block i's spacing)."""
+        stage (``S_blocks[i]`` carries block i's spacing); blocks evolve on
+        their own, so this compares with ``ghosts="evolve"`` only."""
+        if self.ghosts != "evolve":
+            raise ValueError("per-block launches evolve ghosts themselves: use ghosts='evolve'")
         lib = self._lib.load()
         b = self.buffers(U)
         p = self.params
@@ -301,6 +358,34 @@ class BatchedEvolution:
                                              S_blocks[i].data_ptr(), self.ko_sigma, self.ko_order,
                                              p.chi_floor, p.alpha_floor, sx, sy, sz)
                 self._lib.check(rc)
+
+    def constraint_norms(self, U):
+        """Interior L2 norms (H, |M|) over every block's interior points
+        together: each block's norms come from the fused norm kernel
+        (constraints.py:53-62 per block) and are combined weighted by the
+        block's interior point count. With ghost exchange a filled copy of U
+        is measured."""
+        import torch
+        from .fused_rhs import device_scalars, pack_S
+        lib = self._lib.load()
+        if self.ghosts == "exchange":
+            U = U.clone()
+            self.fill(U)
+        need = int(lib.bssn_b200_norms_scratch_bytes())
+        scratch = torch.empty(need // 8 + 1, dtype=torch.float64, device=self.device)
+        out = torch.empty(len(self.pool.blocks), 2, dtype=torch.float64, device=self.device)
+        for i, blk in enumerate(self.pool.blocks):
+            S = device_scalars(pack_S(2.0, 0.0, 1.0, blk.h, 0.0, 1.0, 0.0, (1, 1, 1, 1), (1, 0),
+                                      blk.h, blk.h), self.device)
+            o = int(self.pool.offsets[i])
+            sx, sy, sz = blk.shape
+            rc = lib.bssn_b200_constraint_norms(self._stream(), U[o:].data_ptr(), S.data_ptr(), sx, sy, sz,
+                                                blk.ng, scratch.data_ptr(), need, out[i].data_ptr())
+            self._lib.check(rc)
+        w = torch.tensor([float(b.interior_points) for b in self.pool.blocks], dtype=torch.float64,
+                         device=self.device)
+        hm = torch.sqrt((out ** 2 * w[:, None]).sum(0) / w.sum())
+        return float(hm[0]), float(hm[1])
 
     def block_scalars(self, t: float, dt: float):
         from .fused_rhs import device_scalars, scalars

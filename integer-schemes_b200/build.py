@@ -20,8 +20,8 @@ PKG = HERE / "bssn3d_b200"
 LIB = PKG / "libbssn_b200.so"
 ROOT = HERE.parent
 
-SOURCES = [CSRC / "bssn_b200.cu", CSRC / "ozaki.cu"]
-HEADERS = sorted(CSRC.glob("*.cuh")) + [ROOT / "include" / "bssn_b200.h"]
+SOURCES = [CSRC / "bssn_b200.cu", CSRC / "ozaki.cu", CSRC / "amr_fill.cu"]
+HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "bssn_b200.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

@@ -1,0 +1,183 @@
+// Ghost-zone fill for batched AMR block pools: same-level copies, node-centred
+// 2:1 prolongation from the next coarser level and fine-to-coarse injection,
+// the transfer operators of the reference's node-centred AMR
+// (3D/src/multipatch/amr/kernels.py:52-71 prolongation, :114-145 injection;
+// 3D/src/multipatch/amr/sync.py:70-122 cross-level and same-level fills),
+// applied to the BSSN block pool that the batched stage kernels evolve.
+//
+// A fill is a host-planned list of boxes (bssn_b200_fill_op). One launch
+// executes one list: every thread takes one destination point (flattened
+// over the boxes by a prefix of box volumes, found by binary search) and
+// moves all 24 fields. The work is a gather of a small part of the pool per
+// stage, so the kernel is bound by memory latency and sized to fill the SMs.
+//
+// Prolongation refines the source block x, then y, then z. A point odd on an
+// axis sums its 6 taps in offset order starting from 0 (the reference's
+// `mids = 0.0; mids = mids + w * slice` loop), a point even on an axis takes
+// the coincident node unchanged; every product and sum is rounded
+// separately (no fused multiply-add), so the result equals the sequential
+// whole-block passes bit for bit.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/bssn_b200.h"
+#include "host_util.h"
+
+namespace amr {
+
+constexpr int NFIELD = 24;
+constexpr int NTHREADS = 256;
+
+struct Wmid {
+  double w[6];
+};
+
+__device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
+
+__global__ void __launch_bounds__(NTHREADS) fill_kernel(double* __restrict__ pool,
+                                                        const bssn_b200_fill_op* __restrict__ ops,
+                                                        int nops, long long npoints, const Wmid W) {
+  const long long stride = (long long)gridDim.x * NTHREADS;
+  for (long long p = (long long)blockIdx.x * NTHREADS + threadIdx.x; p < npoints; p += stride) {
+    int lo = 0, hi = nops - 1;  // last op with point0 <= p
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (ops[mid].point0 <= p) lo = mid; else hi = mid - 1;
+    }
+    const bssn_b200_fill_op& op = ops[lo];
+    const int bz = op.hi[2] - op.lo[2], by = op.hi[1] - op.lo[1];
+    long long r = p - op.point0;
+    const int d2 = op.lo[2] + (int)(r % bz);
+    r /= bz;
+    const int d1 = op.lo[1] + (int)(r % by);
+    const int d0 = op.lo[0] + (int)(r / by);
+    if (d0 >= op.hi[0]) continue;  // npoints past the plan's total: nothing to write
+    const int ss0 = op.src_s[0], ss1 = op.src_s[1], ss2 = op.src_s[2];
+    const long long nd = (long long)op.dst_s[0] * op.dst_s[1] * op.dst_s[2];
+    const long long ns = (long long)ss0 * ss1 * ss2;
+    double* dst = pool + op.dst_off + ((long long)d0 * op.dst_s[1] + d1) * op.dst_s[2] + d2;
+    const double* src = pool + op.src_off;
+    if (op.kind != BSSN_B200_FILL_PROLONG) {
+      const int m = op.kind == BSSN_B200_FILL_RESTRICT ? 2 : 1;
+      const long long s = ((long long)(m * d0 + op.shift[0]) * ss1 + (m * d1 + op.shift[1])) * ss2 +
+                          (m * d2 + op.shift[2]);
+#pragma unroll 4
+      for (int f = 0; f < NFIELD; ++f) dst[f * nd] = src[s + f * ns];
+      continue;
+    }
+    // per axis: 1 tap (even, coincident node) or 6 taps (odd, midpoint)
+    const int g0 = d0 + op.shift[0], g1 = d1 + op.shift[1], g2 = d2 + op.shift[2];
+    const bool o0 = g0 & 1, o1 = g1 & 1, o2 = g2 & 1;
+    const int k0 = g0 >> 1, k1 = g1 >> 1, k2 = g2 >> 1;  // arithmetic shift: floor(g / 2)
+    int ix[6], iy[6], iz[6];
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      ix[j] = clampi(o0 ? k0 - 2 + j : k0, ss0 - 1);
+      iy[j] = clampi(o1 ? k1 - 2 + j : k1, ss1 - 1);
+      iz[j] = clampi(o2 ? k2 - 2 + j : k2, ss2 - 1);
+    }
+    const int ny = o1 ? 6 : 1, nz = o2 ? 6 : 1;
+    const long long sxs = (long long)ss1 * ss2;
+    for (int f = 0; f < NFIELD; ++f) {
+      const double* P = src + f * ns;
+      double vz = 0.0;
+      for (int c = 0; c < nz; ++c) {
+        double vy = 0.0;
+        for (int b = 0; b < ny; ++b) {
+          const double* row = P + (long long)iy[b] * ss2 + iz[c];
+          double vx;
+          if (!o0) {
+            vx = row[ix[0] * sxs];
+          } else {
+            vx = 0.0;
+#pragma unroll
+            for (int a = 0; a < 6; ++a) vx = __dadd_rn(vx, __dmul_rn(W.w[a], row[ix[a] * sxs]));
+          }
+          vy = o1 ? __dadd_rn(vy, __dmul_rn(W.w[b], vx)) : vx;
+        }
+        vz = o2 ? __dadd_rn(vz, __dmul_rn(W.w[c], vy)) : vy;
+      }
+      dst[f * nd] = vz;
+    }
+  }
+}
+
+}  // namespace amr
+
+extern "C" {
+
+long long bssn_b200_fill_plan(bssn_b200_fill_op* host_ops, int nops, long long pool_doubles) {
+  using bssn_host::fail;
+  if (!host_ops || nops < 1) {
+    fail(BSSN_B200_EINVAL, "fill_plan: empty op list");
+    return -1;
+  }
+  long long total = 0;
+  for (int i = 0; i < nops; ++i) {
+    bssn_b200_fill_op& op = host_ops[i];
+    const std::string at = "fill_plan: op " + std::to_string(i) + ": ";
+    if (op.kind != BSSN_B200_FILL_COPY && op.kind != BSSN_B200_FILL_RESTRICT && op.kind != BSSN_B200_FILL_PROLONG) {
+      fail(BSSN_B200_EINVAL, at + "unknown kind");
+      return -1;
+    }
+    long long nd = 1, ns = 1, vol = 1;
+    for (int a = 0; a < 3; ++a) {
+      if (op.dst_s[a] < 1 || op.src_s[a] < 1) {
+        fail(BSSN_B200_EINVAL, at + "empty block extent");
+        return -1;
+      }
+      if (op.lo[a] < 0 || op.hi[a] > op.dst_s[a] || op.lo[a] >= op.hi[a]) {
+        fail(BSSN_B200_EINVAL, at + "box outside its destination block or empty");
+        return -1;
+      }
+      if (op.kind != BSSN_B200_FILL_PROLONG) {
+        const long long m = op.kind == BSSN_B200_FILL_RESTRICT ? 2 : 1;
+        const long long s_lo = m * op.lo[a] + op.shift[a], s_hi = m * (op.hi[a] - 1) + op.shift[a];
+        if (s_lo < 0 || s_hi >= op.src_s[a]) {
+          fail(BSSN_B200_EINVAL, at + "source points outside the source block");
+          return -1;
+        }
+      } else if ((long long)op.lo[a] + op.shift[a] < -(1LL << 29) || (long long)op.hi[a] + op.shift[a] > (1LL << 29)) {
+        fail(BSSN_B200_EINVAL, at + "prolongation shift out of range");
+        return -1;
+      }
+      nd *= op.dst_s[a];
+      ns *= op.src_s[a];
+      vol *= op.hi[a] - op.lo[a];
+    }
+    if (op.dst_off < 0 || op.src_off < 0 || op.dst_off + 24 * nd > pool_doubles || op.src_off + 24 * ns > pool_doubles) {
+      fail(BSSN_B200_EINVAL, at + "block outside the pool");
+      return -1;
+    }
+    if (op.dst_off == op.src_off) {
+      fail(BSSN_B200_EINVAL, at + "a block cannot fill itself");
+      return -1;
+    }
+    op.point0 = total;
+    total += vol;
+  }
+  return total;
+}
+
+int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int nops, long long npoints,
+                   const double* wmid) {
+  using bssn_host::fail;
+  if (!pool || !ops || !wmid) return fail(BSSN_B200_EINVAL, "fill: NULL operand");
+  if (nops < 1 || npoints < 1) return fail(BSSN_B200_EINVAL, "fill: empty plan");
+  amr::Wmid W;
+  for (int j = 0; j < 6; ++j) W.w[j] = wmid[j];
+  int sms = 0;
+  int rc = bssn_host::device_sms(&sms);
+  if (rc) return rc;
+  const long long want = (npoints + amr::NTHREADS - 1) / amr::NTHREADS;
+  const int grid = (int)(want < 8LL * sms ? want : 8LL * sms);
+  amr::fill_kernel<<<grid, amr::NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(pool, ops, nops, npoints, W);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return bssn_host::cuda_fail("fill launch", e);
+  return 0;
+}
+
+}  // extern "C"

@@ -29,6 +29,7 @@
 #include <type_traits>
 
 #include "../../include/bssn_b200.h"
+#include "host_util.h"
 #include "stream.cuh"
 
 namespace bssn {
@@ -355,7 +356,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     // ---- tile geometry: the single grid, or the block that owns this tile ----
     long long Sx = args.Sx, Sy = args.Sy, Sz = args.Sz, n = args.n, base = 0;
-    int ntx = args.ntx, nty = args.nty, ntz = args.ntz, lt = tile;
+    int ntx = args.ntx, nty = args.nty, ntz = args.ntz, lt = tile, core = 0;
     Params P = P0;
     if (batched) {
       int lo = 0, hi = args.nblocks - 1;  // last block with tile0 <= tile
@@ -367,7 +368,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
       Sx = bk.sx; Sy = bk.sy; Sz = bk.sz;
       n = Sx * Sy * Sz;
       base = bk.offset;
-      ntx = (bk.sx + TX - 1) / TX; nty = (bk.sy + TY - 1) / TY; ntz = (bk.sz + TZ - 1) / TZ;
+      core = bk.core;  // tiles cover [core, s - core): the ghosts come from a fill
+      ntx = (bk.sx - 2 * core + TX - 1) / TX; nty = (bk.sy - 2 * core + TY - 1) / TY;
+      ntz = (bk.sz - 2 * core + TZ - 1) / TZ;
       lt = tile - bk.tile0;
       P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
       if (lo != cur_block) {
@@ -379,11 +382,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
     if (MODE == MODE_STAGE) P.t = P0.t + cs * P0.dt;  // stage time t, t+dt/2, t+dt/2, t+dt (evolve.py:125-131)
     if (MODE == MODE_MSRK) P.t = P0.t + args.ctime * P0.dt;  // node times t, t+c2 dt, t+c3 dt (evolve.py:139-153)
     const int tz = lt % ntz, ty = (lt / ntz) % nty, tx = lt / (ntz * nty);
-    const long long x0 = (long long)tx * TX, y0 = (long long)ty * TY, z0 = (long long)tz * TZ;
+    const long long x0 = core + (long long)tx * TX, y0 = core + (long long)ty * TY, z0 = core + (long long)tz * TZ;
     const long long gx = x0 + lx, gy = y0 + ly, gz = z0 + lz;
-    const bool inside = gx < Sx && gy < Sy && gz < Sz;
-    // points past the array end compute on clamped data and store nothing
-    const long long gidx = base + (clampll(gx, Sx - 1) * Sy + clampll(gy, Sy - 1)) * Sz + clampll(gz, Sz - 1);
+    const bool inside = gx < Sx - core && gy < Sy - core && gz < Sz - core;
+    // points past the covered range compute on clamped data and store nothing
+    const long long gidx = base + (clampll(gx, Sx - 1 - core) * Sy + clampll(gy, Sy - 1 - core)) * Sz +
+                           clampll(gz, Sz - 1 - core);
     const double* __restrict__ Fbase = args.F + base;
     // Stage this point's 24 values (and, for the RK update, u_n and the
     // accumulator) in shared memory with one batch of cp.async: each thread
@@ -859,6 +863,12 @@ int prepare_batch(bssn::Args* a, const bssn_b200_block* blocks, int nblocks, int
 
 }  // namespace
 
+namespace bssn_host {
+int fail(int code, const std::string& msg) { return ::fail(code, msg); }
+int cuda_fail(const char* what, cudaError_t e) { return ::cuda_fail(what, e); }
+int device_sms(int* sms) { return ::device_sms(sms); }
+}  // namespace bssn_host
+
 extern "C" {
 
 int bssn_b200_batch_plan(bssn_b200_block* host_blocks, int nblocks, int variant) {
@@ -879,8 +889,13 @@ int bssn_b200_batch_plan(bssn_b200_block* host_blocks, int nblocks, int variant)
       fail(BSSN_B200_EINVAL, "batch_plan: block " + std::to_string(b) + " has a bad extent, offset or spacing");
       return -1;
     }
+    if (bk.core < 0 || 2 * bk.core >= bk.sx || 2 * bk.core >= bk.sy || 2 * bk.core >= bk.sz) {
+      fail(BSSN_B200_EINVAL, "batch_plan: block " + std::to_string(b) + " has a core margin that leaves no points");
+      return -1;
+    }
     bk.tile0 = (int)t0;
-    t0 += (long long)((bk.sx + tx - 1) / tx) * ((bk.sy + ty - 1) / ty) * ((bk.sz + tz - 1) / tz);
+    const int c2 = 2 * bk.core;
+    t0 += (long long)((bk.sx - c2 + tx - 1) / tx) * ((bk.sy - c2 + ty - 1) / ty) * ((bk.sz - c2 + tz - 1) / tz);
     if (t0 > (1LL << 30)) {
       fail(BSSN_B200_EINVAL, "batch_plan: too many tiles");
       return -1;
