@@ -84,8 +84,15 @@ typedef struct bssn_b200_fill_op {
 /* Message for the last non-zero status returned on this host thread. */
 const char* bssn_b200_last_error(void);
 
-/* Library version, e.g. "bssn_b200 0.2 sm_100a". */
+/* Library version, e.g. "bssn_b200 0.3 sm_100a". */
 const char* bssn_b200_version(void);
+
+/* Number of bulk-copy waits that gave up since the library was loaded on the
+ * current device (synchronises the device). The stream kernel stages halo
+ * tiles with bulk-tensor copies completing on an mbarrier; each wait is
+ * bounded, and a wait that runs out is counted here (that launch's results
+ * are invalid) instead of hanging the GPU. 0 in a healthy run. */
+int bssn_b200_async_copy_errors(int* count);
 
 /* The BSSN right-hand side: OUT = RHS(F) on every point of the padded grid.
  * Drop-in for the reference's fused FFI handler FusedImpl

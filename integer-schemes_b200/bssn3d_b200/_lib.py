@@ -26,6 +26,7 @@ _SZ = ctypes.c_size_t
 _SIGNATURES = {
     "bssn_b200_last_error": ([], ctypes.c_char_p),
     "bssn_b200_version": ([], ctypes.c_char_p),
+    "bssn_b200_async_copy_errors": ([_P], _I),
     "bssn_b200_rhs": ([_P, _P, _P, _P, _LL, _LL, _LL], _I),
     "bssn_b200_constraints": ([_P, _P, _P, _P, _LL, _LL, _LL], _I),
     "bssn_b200_norms_scratch_bytes": ([], _SZ),

@@ -19,10 +19,12 @@
 // the lowest offset, index clamped at the array ends, mixed second
 // derivatives as a first derivative along the lower axis, then along the
 // higher axis of that result.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <cmath>
 #include <string>
@@ -100,6 +102,50 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// --- bulk-tensor (TMA) loads completing on an mbarrier ----------------------
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Orders this thread's earlier shared-memory accesses before later async-proxy
+// (bulk copy) writes to the same memory.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// One 4-D tile of the tensor map into shared memory (this CTA only; no multicast).
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* map, unsigned long long* bar, int c0,
+                                            int c1, int c2, int c3) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];\n" ::"r"(smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
+// Bounded wait on an mbarrier phase: gives up after kWaitLimit polls and
+// records the failure in g_async_copy_errors instead of spinning forever.
+constexpr long long kWaitLimit = 1LL << 24;
+__device__ int g_async_copy_errors = 0;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  for (long long it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicAdd(&g_async_copy_errors, 1);
+  return false;
+}
+
 // Compile-time loop: body(std::integral_constant<int, I>) for I = B .. E-1, so
 // that every per-field branch and register-array index is resolved statically.
 template <int B, int E>
@@ -121,6 +167,13 @@ struct TileGeom {
   static constexpr int TX = T::X, TY = T::Y, TZ = T::Z;
   static constexpr int HX = TX + 2 * R, HY = TY + 2 * R, HZ = TZ + 2 * R;
   static constexpr int HZP = zpitch(HZ);
+  // With bulk-copy staging a staged row starts ZS_TMA points further down in z
+  // (z0 - R - ZS_TMA), so that the copy starts on a 16-byte boundary when z0 is
+  // even; the copy moves BOXZ points per row (a multiple of 2 doubles).
+  static constexpr int ZS_TMA = R & 1;
+  static constexpr int BOXZ = (HZ + ZS_TMA + 1) / 2 * 2;
+  static_assert(BOXZ <= HZP, "a bulk-copied row must fit the staged z pitch");
+  static constexpr unsigned TMA_BYTES = (unsigned)(BOXZ * HY * HX * sizeof(double));
   static constexpr int SX = HY * HZP, SY = HZP;
   static constexpr int VOL = HX * HY * HZP;   // doubles per staged buffer
   static constexpr int NELEM = HX * HY * HZ;  // staged elements
@@ -135,6 +188,10 @@ struct TileGeom {
   // when it fits next to the tiles in the 227 KB a CTA may use
   static constexpr bool PTS = SMEM + (size_t)3 * NFIELD * NTHREADS * sizeof(double) + 1024 <= 232448;
   static constexpr size_t SMEM_PTS = PTS ? (size_t)3 * NFIELD * NTHREADS * sizeof(double) : 0;
+  // bulk-copy staging keeps NBUF field buffers in flight: a third one (after
+  // the point staging) when it fits, so each copy has two field steps to land
+  static constexpr int NBUF = SMEM + SMEM_PTS + (size_t)VOL * sizeof(double) + 1024 <= 232448 ? 3 : 2;
+  static constexpr size_t SMEM_TMA = SMEM + SMEM_PTS + (NBUF == 3 ? (size_t)VOL * sizeof(double) : 0);
 };
 
 __device__ __forceinline__ Params load_params(const double* __restrict__ S) {
@@ -176,7 +233,7 @@ __device__ __forceinline__ void init_weights(Weights& W, const double* __restric
 
 // Issue the cp.async copies that stage one field's haloed tile, index clamped
 // at the array ends (derivatives.py:83-84 pads with the edge value).
-template <int R, class T = DefaultShape>
+template <int R, class T = DefaultShape, int ZS = 0>
 __device__ __forceinline__ void stage_tile(double* buf, const double* __restrict__ Ff, long long x0,
                                            long long y0, long long z0, long long Sx, long long Sy,
                                            long long Sz, int tid) {
@@ -191,7 +248,7 @@ __device__ __forceinline__ void stage_tile(double* buf, const double* __restrict
       const long long qx = clampll(x0 - R + hx, Sx - 1);
       const long long qy = clampll(y0 - R + hy, Sy - 1);
       const long long qz = clampll(z0 - R + hz, Sz - 1);
-      cp_async8(buf + hx * Geo::SX + hy * Geo::SY + hz, Ff + (qx * Sy + qy) * Sz + qz);
+      cp_async8(buf + hx * Geo::SX + hy * Geo::SY + hz + ZS, Ff + (qx * Sy + qy) * Sz + qz);
     }
   }
 }
@@ -321,13 +378,17 @@ __device__ __forceinline__ void enforce_point(double* en, double* O, long long n
 // ---------------------------------------------------------------------------
 // The streaming fused kernel.
 // ---------------------------------------------------------------------------
-template <int R, int MODE, class T = DefaultShape>
-__global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
+// TMA = true: every tile's halo box is staged by bulk-tensor copies (the
+// array is a single grid whose layout allows them); false: per-thread clamped
+// cp.async staging (batched block pools, odd z extents). One path per
+// instantiation keeps the unrolled field loop small in the instruction cache.
+template <int R, int MODE, class T = DefaultShape, bool TMA = false>
+__global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, const __grid_constant__ CUtensorMap tmF) {
   using Geo = TileGeom<R, T>;
   constexpr int TX = Geo::TX, TY = Geo::TY, TZ = Geo::TZ, HZP = Geo::TP;
   constexpr bool RATES = MODE != MODE_CON && MODE != MODE_NORM;
   constexpr bool CONS = MODE == MODE_CON || MODE == MODE_NORM;
-  extern __shared__ __align__(16) double smem[];
+  extern __shared__ __align__(128) double smem[];
   double* const buf0 = smem;
   double* const buf1 = smem + Geo::VOL;
   double* const T1 = smem + 2 * Geo::VOL;
@@ -336,12 +397,33 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
   double* const pU = pY + NFIELD * NTHREADS;  // [24][256] u_n (stage mode)
   double* const pA = pU + NFIELD * NTHREADS;  // [24][256] accumulator (stages 1-3)
   __shared__ Weights W;
+  __shared__ __align__(8) unsigned long long tbar[3];  // bulk-copy completion, one per buffer
+  constexpr int NB = TMA ? Geo::NBUF : 2;
+  double* const buf2 = T2 + Geo::T2VOL + (Geo::PTS ? 3 * NFIELD * NTHREADS : 0);  // TMA with NBUF 3 only
+  auto bufp = [&](int b) -> double* { return b == 0 ? buf0 : (b == 1 ? buf1 : buf2); };
 
   const int tid = threadIdx.x;
   const bool batched = args.blocks != nullptr;
   const int lz = tid % TZ, ly = (tid / TZ) % TY, lx = tid / (TZ * TY);
-  const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R);
+  constexpr int ZS = TMA ? Geo::ZS_TMA : 0;  // z shift of the staged rows
+  const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R + ZS);
   constexpr int st[3] = {Geo::SX, Geo::SY, 1};
+  unsigned tphase = 0;    // bit b: parity of the next completion of tbar[b]
+  unsigned tpending = 0;  // bit b: a copy into buffer b is in flight
+  bool tfailed = false;   // this thread gave up on a wait: skip the rest
+  if (TMA) {
+    // bulk-tensor destinations must start on 128-byte boundaries: refuse to
+    // run (and count the error) rather than issue a misaligned copy
+    if (smem_addr(smem) & 127u) {
+      if (tid == 0) atomicAdd(&g_async_copy_errors, 1);
+      return;
+    }
+    if (tid == 0) {
+      for (int b = 0; b < NB; ++b) mbar_init(&tbar[b], 1);
+      asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+  }
   const int ntiles = batched ? args.ntiles : args.ntx * args.nty * args.ntz;
   const bool use_ko = RATES && args.use_ko != 0;
   const Params P0 = load_params(args.S);
@@ -415,21 +497,75 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
     Stream<RATES, CONS> acc;
     acc.init(fld);
 
-    stage_tile<R, T>(buf0, Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
-    cp_async_commit();
+    // Bulk-copy staging: thread 0 issues one tensor copy of the halo box per
+    // field (the copy fills cells past the array with zeros; on edge tiles
+    // the rows are then fixed up to the clamped values).
+    const int bz0 = (int)z0 - R - ZS;
+    const int bx0 = (int)x0 - R, by0 = (int)y0 - R;
+    const bool edge = bx0 < 0 || bx0 + Geo::HX > Sx || by0 < 0 || by0 + Geo::HY > Sy || bz0 < 0 ||
+                      bz0 + Geo::BOXZ > Sz;
+    auto tma_issue = [&](int field, int b) {
+      if (tid == 0) {
+        mbar_expect_tx(&tbar[b], Geo::TMA_BYTES);
+        tma_load_4d(bufp(b), &tmF, &tbar[b], bz0, by0, bx0, field);
+      }
+      tpending |= 1u << b;
+    };
+    // Edge clamp of a bulk-copied box (derivatives.py:83-84 edge padding):
+    // thread r < HX*HY owns row r; a row outside the array in x or y copies
+    // the clamped in-array row, and cells past the z ends take the clamped
+    // z value. Reads touch only cells inside the array, which no thread writes.
+    auto clamp_box = [&](double* buf) {
+      if (tid < Geo::HX * Geo::HY) {
+        const int hy = tid % Geo::HY, hx = tid / Geo::HY;
+        const int X = bx0 + hx, Y = by0 + hy;
+        const int cx = X < 0 ? 0 : (X >= Sx ? (int)Sx - 1 : X);
+        const int cy = Y < 0 ? 0 : (Y >= Sy ? (int)Sy - 1 : Y);
+        double* dst = buf + hx * Geo::SX + hy * Geo::SY;
+        const double* src = buf + (cx - bx0) * Geo::SX + (cy - by0) * Geo::SY;
+        const int zlo = bz0 < 0 ? -bz0 : 0;                                       // first in-array cell
+        const int zhi = bz0 + Geo::BOXZ > Sz ? (int)Sz - bz0 : Geo::BOXZ;          // one past the last
+        const bool whole = cx != X || cy != Y;
+        for (int hz = 0; hz < Geo::BOXZ; ++hz) {
+          const int q = hz < zlo ? zlo : (hz >= zhi ? zhi - 1 : hz);
+          if (whole || q != hz) dst[hz] = src[q];
+        }
+      }
+    };
+    if (TMA) {
+      for (int q = 0; q < NB - 1; ++q) tma_issue(stream_field(q), q);
+    } else {
+      stage_tile<R, T, ZS>(buf0, Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
+      cp_async_commit();
+    }
     Unroll<0, NFIELD>::run([&](auto ic) {
       constexpr int idx = decltype(ic)::value;
       constexpr int f = stream_field(idx);
-      const double* __restrict__ cur = (idx & 1) ? buf1 : buf0;
-      if (idx + 1 < NFIELD) {
-        stage_tile<R, T>((idx & 1) ? buf0 : buf1, Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
-                         Sx, Sy, Sz, tid);
-        cp_async_commit();
-        cp_async_wait<1>();
+      constexpr int b = idx % NB;
+      const double* __restrict__ cur = bufp(b);
+      if (TMA) {
+        // the buffer of field idx - 1 is free (the field step ended in a barrier)
+        if (idx + NB - 1 < NFIELD) tma_issue(stream_field(idx + NB - 1), (idx + NB - 1) % NB);
+        if (idx == NFIELD - 1) cp_async_wait<0>();  // the point staging of u_n / accumulator
+        if (!tfailed && mbar_wait_bounded(&tbar[b], (tphase >> b) & 1u)) tpending &= ~(1u << b);
+        else tfailed = true;  // results of this CTA are garbage; the error count says so
+        tphase ^= 1u << b;
+        if (edge) {
+          clamp_box(bufp(b));
+          fence_proxy_async();  // these writes before the next bulk copy into the buffer
+          __syncthreads();
+        }
       } else {
-        cp_async_wait<0>();
+        if (idx + 1 < NFIELD) {
+          stage_tile<R, T, ZS>((idx & 1) ? buf0 : buf1, Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
+                           Sx, Sy, Sz, tid);
+          cp_async_commit();
+          cp_async_wait<1>();
+        } else {
+          cp_async_wait<0>();
+        }
+        __syncthreads();
       }
-      __syncthreads();
 
       // axial taps: first derivative, diagonal second derivative, KO
       double d1[3], d2[6], ko = 0.0;
@@ -462,7 +598,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           const int zz = e % (TZ + 6);
           const int yy = (e / (TZ + 6)) % Geo::T1Y;
           const int xx = e / ((TZ + 6) * Geo::T1Y);
-          const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R);
+          const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R + ZS);
           double s = 0.0;
 #pragma unroll
           for (int k = 0; k < 7; ++k)
@@ -474,7 +610,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
           const int zz = e % (TZ + 6);
           const int yy = (e / (TZ + 6)) % TY;
           const int xx = e / ((TZ + 6) * TY);
-          const int cc = (xx + R) * Geo::SX + (yy + R) * Geo::SY + (zz - 3 + R);
+          const int cc = (xx + R) * Geo::SX + (yy + R) * Geo::SY + (zz - 3 + R + ZS);
           double s = 0.0;
 #pragma unroll
           for (int k = 0; k < 7; ++k)
@@ -597,6 +733,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args) {
       acc.finalize(fld, P, emit, NoCon());
       if (stage == 2 && inside) enforce_point(en, O, n, args.chi_floor, args.alpha_floor);
     }
+  }
+  if (TMA && tfailed) {
+    // give copies still in flight a bounded time to land before the CTA exits
+    for (int b = 0; b < NB; ++b)
+      if (tpending & (1u << b)) mbar_wait_bounded(&tbar[b], ((tphase >> b) & 1u) ^ 1u);
   }
   if (MODE == MODE_NORM) {
     // fixed-order block reduction of the per-thread sums (reuses the staging buffer)
@@ -775,15 +916,83 @@ int set_smem(K kern, size_t smem, int* flags) {
   return 0;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiled encode_tiled() {
+  static EncodeTiled fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return static_cast<EncodeTiled>(nullptr);
+    return reinterpret_cast<EncodeTiled>(p);
+  }();
+  return fn;
+}
+
+// Tensor map of a (24, Sx, Sy, Sz) float64 state for the stream kernel's halo
+// boxes (BOXZ x HY x HX x 1 field). False when the layout does not allow bulk
+// copies: every stride must be a multiple of 16 bytes (Sz even) and the base
+// 16-byte aligned; the kernel then stages every tile with cp.async.
+template <int R, class T>
+bool make_state_map(CUtensorMap* map, const double* F, long long Sx, long long Sy, long long Sz) {
+#ifdef BSSN_B200_NO_TMA
+  (void)map; (void)F; (void)Sx; (void)Sy; (void)Sz;
+  return false;
+#else
+  using Geo = bssn::TileGeom<R, T>;
+  EncodeTiled enc = encode_tiled();
+  if (Geo::BOXZ != Geo::HZP) return false;  // a copied box row must be exactly one staged row
+  if (!enc || (Sz & 1) || (reinterpret_cast<uintptr_t>(F) & 15)) return false;
+  if (Sx < Geo::HX || Sy < Geo::HY || Sz < Geo::BOXZ) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)Sz, (cuuint64_t)Sy, (cuuint64_t)Sx, (cuuint64_t)bssn::NFIELD};
+  const cuuint64_t strides[3] = {(cuuint64_t)Sz * 8, (cuuint64_t)(Sy * Sz) * 8, (cuuint64_t)(Sx * Sy * Sz) * 8};
+  const cuuint32_t box[4] = {(cuuint32_t)Geo::BOXZ, (cuuint32_t)Geo::HY, (cuuint32_t)Geo::HX, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(F), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+#endif
+}
+
+// Halo staging of the single-grid stream kernel: per-thread clamped cp.async
+// copies (default), or bulk-tensor copies when BSSN_B200_STAGING=tma and the
+// layout allows them. Read on every call, like the reference's FFI handler
+// reads its environment knobs (3D/src/bssn3d/cuda/rhs_fused.cu:34-41). Both
+// give the same bytes; on B200 the per-thread form measured faster for this
+// kernel (its warps stay in step through the unrolled field loop).
+bool tma_staging_requested() {
+  const char* v = std::getenv("BSSN_B200_STAGING");
+  return v != nullptr && std::strcmp(v, "tma") == 0;
+}
+
 template <int R, int MODE, class T = bssn::DefaultShape>
 int launch_stream(const bssn::Args& a, cudaStream_t stream, int grid) {
   using Geo = bssn::TileGeom<R, T>;
   const size_t smem = Geo::SMEM + Geo::SMEM_PTS;
-  auto kern = bssn::stream_kernel<R, MODE, T>;
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  if constexpr (std::is_same<T, bssn::DefaultShape>::value) {
+    if (!a.blocks && tma_staging_requested() && make_state_map<R, T>(&map, a.F, a.Sx, a.Sy, a.Sz)) {
+      const size_t smem_tma = Geo::SMEM_TMA;
+      auto kern = bssn::stream_kernel<R, MODE, T, true>;
+      static int flags[kMaxDev] = {0};
+      int rc = set_smem(kern, smem_tma, flags);
+      if (rc) return rc;
+      kern<<<grid, bssn::NTHREADS, smem_tma, stream>>>(a, map);
+      cudaError_t e = cudaGetLastError();
+      if (e != cudaSuccess) return cuda_fail("stream kernel launch", e);
+      return 0;
+    }
+  }
+  auto kern = bssn::stream_kernel<R, MODE, T, false>;
   static int flags[kMaxDev] = {0};
   int rc = set_smem(kern, smem, flags);
   if (rc) return rc;
-  kern<<<grid, bssn::NTHREADS, smem, stream>>>(a);
+  kern<<<grid, bssn::NTHREADS, smem, stream>>>(a, map);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail("stream kernel launch", e);
   return 0;
@@ -943,7 +1152,14 @@ int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const do
 
 const char* bssn_b200_last_error(void) { return g_err.c_str(); }
 
-const char* bssn_b200_version(void) { return "bssn_b200 0.2 sm_100a"; }
+const char* bssn_b200_version(void) { return "bssn_b200 0.3 sm_100a"; }
+
+int bssn_b200_async_copy_errors(int* count) {
+  if (!count) return fail(BSSN_B200_EINVAL, "async_copy_errors: NULL operand");
+  cudaError_t e = cudaMemcpyFromSymbol(count, bssn::g_async_copy_errors, sizeof(int));
+  if (e != cudaSuccess) return cuda_fail("async_copy_errors", e);
+  return 0;
+}
 
 int bssn_b200_rhs(void* stream, const double* F, const double* S, double* OUT, long long Sx,
                   long long Sy, long long Sz) {

@@ -196,7 +196,15 @@ def test_exchange_variants_agree_and_rhs_fills_first():
     for i, (G, blk) in enumerate(zip(A.geometry_of(pool), pool.blocks)):
         I = (slice(None),) + (slice(G.ng, -G.ng),) * 3
         ref = O.rhs(G.view(filled), _S(blk.h, dt, 0.0))[I]
-        assert O.normwise_rel(G.view(r)[I], ref).max() < 1e-12, i
+        # Where a rate is pure cancellation (chi's CAHD term on a block far from
+        # the punctures is ~1e-8 of its terms) two correct evaluations differ by
+        # more than 1e-12 of the result; the bar is then what the oracle and the
+        # reference's compiled algebra themselves agree to.
+        bar = np.full(24, 1e-12)
+        if O.have_ref():
+            other = O.ref_rhs(G.view(filled), _S(blk.h, dt, 0.0))[I]
+            bar = np.maximum(bar, 4.0 * O.normwise_rel(ref, other))
+        assert np.all(O.normwise_rel(G.view(r)[I], ref) <= bar), i
 
 
 def test_workload_exchange_steps_stay_finite_with_constraint_norms():
