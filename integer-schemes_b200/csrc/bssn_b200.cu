@@ -84,11 +84,12 @@ struct Weights {
   double wko[3][9];
 };
 
-// Stencil sums are evaluated with separately rounded products and sums, tap
-// by tap from the lowest offset: the same IEEE operations as the reference's
-// `sum(stencil[k] * slice_k)` (derivatives.py:78-88), so the GPU derivatives
-// are bit-identical to it (no FMA contraction).
-__device__ __forceinline__ double tap(double acc, double w, double v) { return __dadd_rn(acc, __dmul_rn(w, v)); }
+// Stencil sums are evaluated tap by tap from the lowest offset
+// (derivatives.py:78-88), each tap one fused multiply-add, the contraction the
+// reference's own CUDA kernel is compiled with. IEEE fma is exactly rounded,
+// so the CPU oracle (which uses fma() in the same order) reproduces every
+// derivative bit for bit.
+__device__ __forceinline__ double tap(double acc, double w, double v) { return __fma_rn(w, v, acc); }
 
 __device__ __forceinline__ long long clampll(long long v, long long hi) {
   return v < 0 ? 0 : (v > hi ? hi : v);

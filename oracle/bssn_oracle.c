@@ -66,7 +66,10 @@ static inline long clampl(long v, long lo, long hi) {
 
 /* One pass of a centred stencil along `axis` of a (Sx,Sy,Sz) array:
  * out = sum_k (coef[k]/den*factor) * in[clamp(p + k - reach)], summed in tap
- * order from the lowest offset, like derivatives.py:78-88. */
+ * order from the lowest offset, like derivatives.py:78-88, each tap one fused
+ * multiply-add (the contraction the reference's CUDA kernel is compiled with,
+ * 3D/src/bssn3d/cuda/rhs_fused.cu; IEEE fma is exactly rounded, so the GPU
+ * taps reproduce these values bit for bit). */
 static void apply_axis(const double* in, double* out, const long S[3], int axis,
                        const double* coef, int ntap, double den, double factor) {
   const int reach = (ntap - 1) / 2;
@@ -85,7 +88,7 @@ static void apply_axis(const double* in, double* out, const long S[3], int axis,
         double acc = 0.0;
         for (int k = 0; k < ntap; ++k) {
           long q = clampl(pa + k - reach, 0, S[axis] - 1);
-          acc += w[k] * in[off0 + q * stride[axis]];
+          acc = fma(w[k], in[off0 + q * stride[axis]], acc);
         }
         out[base] = acc;
       }
