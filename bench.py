@@ -56,6 +56,16 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128, help="interior points per axis")
+    ap.add_argument("--workload", default="bl128", choices=["bl128", "amr3", "amr4"],
+                    help="bl128: one uniform block (default, --n sets its size); amr3/amr4: the "
+                         "600- and 2000-block Brill-Lindquist block lists")
+    ap.add_argument("--integrator", default="rk4", choices=["rk4", "rk4_2_1", "rk4_2_2"],
+                    help="uniform workload: RK4 or a 2-step/3-stage MSRK integrator")
+    ap.add_argument("--ghosts", default="exchange", choices=["exchange", "evolve"],
+                    help="block lists: refill ghosts from other blocks each stage, or evolve them")
+    ap.add_argument("--track", type=int, default=0,
+                    help="after timing, evolve this many more steps and record the constraint norms")
+    ap.add_argument("--track-every", type=int, default=10)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
@@ -257,10 +267,22 @@ def bench_b200(args):
     grid, U_host, dt = ID.workload(1, n=args.n)
     interior = grid.interior_points
     npts = int(np.prod(grid.shape))
-    evo = BSSNEvolution(grid, ko_sigma=0.1, bc="none", ko_order=6)
+    msrk = args.integrator != "rk4"
+    nstage = 3 if msrk else 4
+    evo = BSSNEvolution(grid, ko_sigma=0.1, bc="none", ko_order=6, integrator=args.integrator)
     U0 = torch.from_numpy(U_host).to(dev)
     S0 = evo._S(0.0, dt, dev)
-    graph, U_g, S_g = evo.capture(U0, S0)
+    if msrk:
+        # the RK4 start that keeps f(y_0), then the MSRK step captured as a graph
+        KP = torch.empty_like(U0)
+        U1 = U0.clone()
+        evo._startup_inplace(U1, KP, S0)
+        evo._advance_time(S0)
+        graph, U_g, S_g, K_g = evo.capture_msrk(U1, S0, KP)
+        args.no_stage_timing = True
+        args.no_e2e = True
+    else:
+        graph, U_g, S_g = evo.capture(U0, S0)
 
     def barrier():
         if world > 1:
@@ -289,6 +311,27 @@ def bench_b200(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     finite = bool(torch.isfinite(U_g).all().item())
+    tracked = None
+    if args.track > 0:
+        # a fresh run from t = 0 on its own captured step
+        from bssn3d_b200.constraints import ConstraintSolver
+        cs = ConstraintSolver(grid)
+        S2 = evo._S(0.0, dt, dev)
+        if msrk:
+            K2, U2 = torch.empty_like(U0), U0.clone()
+            evo._startup_inplace(U2, K2, S2)
+            evo._advance_time(S2)
+            g2, U2g, S2g, K2g = evo.capture_msrk(U2, S2, K2)   # the state after the RK4 start
+        else:
+            g2, U2g, S2g = evo.capture(U0, S2)
+
+        def advance(k):
+            for _ in range(k):
+                g2.replay()
+        offset = 1 if msrk else 0
+        tracked = [[r[0] + offset] + r[1:]
+                   for r in track_constraints(advance, lambda: cs.l2(U2g), args.track, args.track_every)]
+        del g2
 
     # per-launch stage-kernel durations (roofline), on the launching stream
     stage_ms = []
@@ -340,7 +383,7 @@ def bench_b200(args):
     fp64_peak = measure_fp64_peak(torch, dev) if (rank == 0 and not args.no_fp64_peak) else None
 
     value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
-    mean_stage = statistics.mean(stage_ms[:3]) if stage_ms else ms / args.steps / 4
+    mean_stage = statistics.mean(stage_ms[:3]) if stage_ms else ms / args.steps / nstage
     achieved_gbs = npts * STAGE_BYTES / (mean_stage * 1e-3) / 1e9
     flops = npts * (FLOPS_PER_POINT + KO_FLOPS_PER_POINT)
     achieved_tf = flops / (mean_stage * 1e-3) / 1e12
@@ -367,18 +410,128 @@ def bench_b200(args):
         except (FileNotFoundError, OSError) as exc:
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                    "sample": f"unavailable: {exc}"}
+    metric = METRIC
+    if msrk:
+        # a step advances the solution as far as an RK4 step: count it like one
+        metric = f"BSSN RK4-equivalent Mpoint-updates/s ({args.integrator} MSRK step, fused FP64)"
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "metric": metric, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": f"Brill-Lindquist q=1/10, {args.n}^3 interior +3 ghosts on [-8,8]^3, "
-                               f"RK4 step (4 fused RHS+KO+stage launches), KO sigma 0.1 order 6",
+                               + (f"{args.integrator} MSRK step (3 fused RHS+KO+stage launches)" if msrk else
+                                  "RK4 step (4 fused RHS+KO+stage launches)") + ", KO sigma 0.1 order 6",
+                   "integrator": args.integrator,
                    "array": list(grid.shape), "state_bytes": int(U_host.nbytes),
                    "l2": "inputs larger than L2 (462 MB state)", "parallelism": f"replicas x{world}"},
-        "clocks": clk, "gpu_launches": 5 * args.steps, "finite": finite,
+        "clocks": clk, "gpu_launches": (nstage + 1) * args.steps, "finite": finite,
         "stage_ms": stage_ms, "roofline": roofline, "roofline_fp64": roofline_fp64,
         "e2e": e2e, "cpu_baseline": cpu,
+    }
+    if tracked is not None:
+        line["constraints"] = tracked
+    del graph
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def track_constraints(advance, norms, total: int, every: int):
+    """[[steps, H, M], ...]: the interior constraint norms at step 0 and after
+    every ``every`` further steps, ``total`` steps in all."""
+    out = [[0] + list(norms())]
+    done = 0
+    while done < total:
+        k = min(every, total - done)
+        advance(k)
+        done += k
+        out.append([done] + list(norms()))
+    return out
+
+
+def bench_amr(args):
+    """A block-list workload: one persistent stage launch per RK4 stage over
+    every block (plus the ghost fill per level with ghosts="exchange"), the
+    step captured as a graph; value counts 4 point-updates per interior point
+    per step. Replicas under torchrun."""
+    import torch
+    world, rank, local = dist_env()
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from bssn3d_b200 import amr
+
+    index = int(args.workload[-1])
+    blocks, punct, dt = amr.workload(index)
+    pool = amr.BlockPool(blocks)
+    U0 = torch.from_numpy(pool.initial_state(punct, seed=0)).to(dev)
+    t_plan = time.time()
+    evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=0, device=dev, ghosts=args.ghosts)
+    t_plan = time.time() - t_plan
+    tune = amr.autotune(evo, U0, dt)
+    graph, U_g, S_g = evo.capture(U0, evo.scalars(0.0, dt))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    for _ in range(args.warmup):
+        graph.replay()
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        graph.replay()
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    finite = bool(torch.isfinite(U_g).all().item())
+    interior = pool.interior_points
+    value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
+    fills = len(evo.dplan.fill) if evo.dplan is not None else 0
+    tracked = None
+    if args.track > 0:
+        # a fresh run from t = 0 on its own captured step
+        g2, U2g, S2g = evo.capture(U0, evo.scalars(0.0, dt))
+
+        def advance(k):
+            for _ in range(k):
+                g2.replay()
+        tracked = track_constraints(advance, lambda: evo.constraint_norms(U2g), args.track, args.track_every)
+        del g2
+    line = {
+        "metric": METRIC.replace("RK4 step", "RK4 step over a block list"), "value": value, "unit": UNIT,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{len(blocks)} Brill-Lindquist blocks, {len(set(b.level for b in blocks))} levels "
+                               f"(amr.workload({index})), interiors 16^3/24^3/32^3 +3 ghosts",
+                   "ghosts": args.ghosts, "interior_points": interior, "points": pool.points,
+                   "state_bytes": int(pool.size * 8), "variant": evo.variant,
+                   "autotune_ms": {str(k): v for k, v in tune.items()},
+                   "plan_s": round(t_plan, 2), "parallelism": f"replicas x{world}"},
+        "clocks": clk, "gpu_launches": (4 * (1 + fills) + 1) * args.steps, "finite": finite,
+        "ghost_points": evo.plan.counts if evo.plan is not None else None,
+        "constraints": tracked, "roofline": None, "e2e": None, "cpu_baseline": None,
     }
     del graph
     if world > 1:
@@ -392,6 +545,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
+    elif args.workload.startswith("amr"):
+        bench_amr(args)
     else:
         bench_b200(args)
 

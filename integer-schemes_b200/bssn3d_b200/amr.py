@@ -328,6 +328,9 @@ class BatchedEvolution:
         with torch.cuda.graph(g):
             self.step_inplace(U_g, S_g)
             self.advance_time(S_g)
+        # a graph does not own the memory it replays on: keep its static
+        # tensors, stage buffers and plan tables alive with the graph object
+        g.static_tensors = (U_g, S_g, self.buffers(U_g), self.table_dev, self.dplan)
         return g, U_g, S_g
 
     def evolve(self, U, dt: float, nsteps: int, t0: float = 0.0):

@@ -220,6 +220,9 @@ class BSSNEvolution:
         with torch.cuda.graph(graph):
             self._step_inplace(U_g, S_g)
             self._advance_time(S_g)
+        # a graph does not own the memory it replays on: keep its static
+        # tensors and stage buffers alive as long as the graph object is
+        graph.static_tensors = (U_g, S_g, self._buffers(U_g))
         return graph, U_g, S_g
 
     def capture_msrk(self, U: torch.Tensor, S: torch.Tensor, KP: torch.Tensor):
@@ -240,4 +243,5 @@ class BSSNEvolution:
         with torch.cuda.graph(graph):
             self._msrk_step_inplace(U_g, K_g, S_g)
             self._advance_time(S_g)
+        graph.static_tensors = (U_g, S_g, K_g, self._buffers(U_g))
         return graph, U_g, S_g, K_g

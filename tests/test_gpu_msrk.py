@@ -144,3 +144,26 @@ def test_msrk_stage_rejects_bad_operands_without_launching():
     assert "msrk_stage" in lib.bssn_b200_last_error().decode()
     torch.cuda.synchronize()
     assert torch.equal(A, before)
+
+
+def test_captured_graph_keeps_its_tensors_alive():
+    """A graph replays on fixed addresses: the tensors it was captured on must
+    outlive it even when the caller drops them and the memory is reused."""
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.state import BSSNState
+    grid, U, dt = ID.workload(1, n=16)
+    evo = _evo(grid, "rk4_2_2", ko=0.1, bc="none", ko_order=6)
+    U0 = torch.from_numpy(U).cuda()
+    ref = evo.evolve(BSSNState(U0), dt, 6).data.clone()
+    S = evo._S(0.0, dt, U0.device)
+    KP, U1 = torch.empty_like(U0), U0.clone()
+    evo._startup_inplace(U1, KP, S)
+    evo._advance_time(S)
+    g, Ug, _, _ = evo.capture_msrk(U1, S, KP)
+    del KP, S
+    junk = []
+    for _ in range(5):
+        junk.append(torch.full_like(U0, float("nan")))
+        junk.append(torch.full((16,), float("nan"), dtype=torch.float64, device="cuda"))
+        g.replay()
+    assert torch.equal(Ug, ref)
