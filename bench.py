@@ -56,9 +56,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--n", type=int, default=128, help="interior points per axis")
-    ap.add_argument("--workload", default="bl128", choices=["bl128", "amr3", "amr4"],
+    ap.add_argument("--workload", default="bl128", choices=["bl128", "amr3", "amr4", "ozaki192"],
                     help="bl128: one uniform block (default, --n sets its size); amr3/amr4: the "
-                         "600- and 2000-block Brill-Lindquist block lists")
+                         "600- and 2000-block Brill-Lindquist block lists; ozaki192: the RHS with "
+                         "INT8 tensor-core derivatives on the 192^3 block, k = 5..8")
     ap.add_argument("--integrator", default="rk4", choices=["rk4", "rk4_2_1", "rk4_2_2"],
                     help="uniform workload: RK4 or a 2-step/3-stage MSRK integrator")
     ap.add_argument("--ghosts", default="exchange", choices=["exchange", "evolve"],
@@ -541,12 +542,80 @@ def bench_amr(args):
         print(json.dumps(line), flush=True)
 
 
+def bench_ozaki(args):
+    """RHS with Ozaki INT8 derivatives (k digit planes, tcgen05 kind::i8) and
+    the float64 algebra on the 192^3 q=1/10 block, against the fused float64
+    RHS of the same state: time per RHS, per-field normwise error, and
+    bit-identity over 5 repeated runs, for k = 5..8. value = the smallest k
+    whose worst field error is <= 1e-10."""
+    import torch
+    dev = torch.device("cuda:0")
+    torch.cuda.set_device(dev)
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.fused_rhs import device_scalars, pack_S, rhs_tensor
+    from bssn3d_b200.ozaki import OzakiDerivatives
+    grid, U_host, dt = ID.workload(2)
+    U = torch.from_numpy(U_host).to(dev)
+    S = device_scalars(pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0),
+                              grid.dy, grid.dz), dev)
+    interior = grid.interior_points
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn, reps):
+        for _ in range(max(args.warmup, 1)):
+            fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
+
+    ref = rhs_tensor(U, S)
+    fp64_ms = timed(lambda: rhs_tensor(U, S), args.steps)
+    den = ref.reshape(24, -1).abs().amax(dim=1)
+    sweep = {}
+    chosen = None
+    for k in (5, 6, 7, 8):
+        oz = OzakiDerivatives(U.shape[1:], k, device=dev)
+        ms = timed(lambda: oz.rhs(U, S), args.steps)
+        out = oz.rhs(U, S)
+        oz.check()
+        num = (out - ref).reshape(24, -1).abs().amax(dim=1)
+        err = torch.where(num == 0, torch.zeros_like(num), num / den.clamp_min(1e-300))
+        same = all(torch.equal(oz.rhs(U, S), out) for _ in range(4))
+        sweep[str(k)] = {"ms_per_rhs": ms, "max_field_err": float(err.max()), "worst_field": int(err.argmax()),
+                         "bit_identical_5_runs": same,
+                         "mpoint_updates_per_s": interior / (ms * 1e-3) / 1e6}
+        if chosen is None and float(err.max()) <= 1e-10:
+            chosen = k
+        del oz, out
+        torch.cuda.empty_cache()
+    k = chosen if chosen is not None else 8
+    line = {
+        "metric": f"BSSN RHS Mpoint-updates/s (Ozaki INT8 derivatives k={k} + FP64 algebra)",
+        "value": sweep[str(k)]["mpoint_updates_per_s"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sweep[str(k)]["ms_per_rhs"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "i8 digits, i32 accumulation, f64 algebra",
+        "data": "synthetic",
+        "config": {"workload": "Brill-Lindquist q=1/10, 192^3 interior +3 ghosts on [-8,8]^3, one RHS",
+                   "array": list(grid.shape), "k_chosen_for_1e-10": chosen},
+        "fp64_fused": {"ms_per_rhs": fp64_ms, "mpoint_updates_per_s": interior / (fp64_ms * 1e-3) / 1e6},
+        "sweep": sweep, "roofline": None, "e2e": None, "cpu_baseline": None,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         bench_reference(args)
     elif args.workload.startswith("amr"):
         bench_amr(args)
+    elif args.workload == "ozaki192":
+        bench_ozaki(args)
     else:
         bench_b200(args)
 
