@@ -181,18 +181,24 @@ struct TileGeom {
   static constexpr int PER_THREAD = (NELEM + NTHREADS - 1) / NTHREADS;
   // separable mixed-derivative passes
   static constexpr int TP = zpitch(TZ + 6);                       // z pitch of T1/T2
-  static constexpr int T1Y = TY + 6, T1N = TX * T1Y * (TZ + 6);  // d/dx over y and z halos
-  static constexpr int T2N = TX * TY * (TZ + 6);                 // d/dy over the z halo
+  // The T1/T2 passes walk rows of TROW points (the TZ + 6 needed, padded) so
+  // that 16 consecutive threads touch 16 consecutive doubles: a whole pitch
+  // (rows back to back) or exactly 16; the extra columns are never read.
+  static constexpr int TROW = TZ + 6 <= 16 ? 16 : TP;
+  static_assert(TROW <= TP, "T rows fit the pitch");
+  static constexpr int T1Y = TY + 6, T1N = TX * T1Y * TROW;  // d/dx over y and z halos
+  static constexpr int T2N = TX * TY * TROW;                 // d/dy over the z halo
   static constexpr int T1VOL = TX * T1Y * TP, T2VOL = TX * TY * TP;
   static constexpr size_t SMEM = (2 * (size_t)VOL + T1VOL + T2VOL) * sizeof(double);
   // + per-point staging of the stage input, u_n and the accumulator (24 each),
   // when it fits next to the tiles in the 227 KB a CTA may use
   static constexpr bool PTS = SMEM + (size_t)3 * NFIELD * NTHREADS * sizeof(double) + 1024 <= 232448;
   static constexpr size_t SMEM_PTS = PTS ? (size_t)3 * NFIELD * NTHREADS * sizeof(double) : 0;
-  // bulk-copy staging keeps NBUF field buffers in flight: a third one (after
-  // the point staging) when it fits, so each copy has two field steps to land
-  static constexpr int NBUF = SMEM + SMEM_PTS + (size_t)VOL * sizeof(double) + 1024 <= 232448 ? 3 : 2;
-  static constexpr size_t SMEM_TMA = SMEM + SMEM_PTS + (NBUF == 3 ? (size_t)VOL * sizeof(double) : 0);
+  // Three rotating buffers fit next to the point staging for R = 3, but the
+  // shared memory they take comes out of the L1 that holds the register
+  // spills: measured 2-6 % slower on B200, so the staging rotates two.
+  static constexpr int NBUF = 2;
+  static constexpr size_t SMEM_RUN = SMEM + SMEM_PTS + (NBUF == 3 ? (size_t)VOL * sizeof(double) : 0);
 };
 
 __device__ __forceinline__ Params load_params(const double* __restrict__ S) {
@@ -399,14 +405,21 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
   double* const pA = pU + NFIELD * NTHREADS;  // [24][256] accumulator (stages 1-3)
   __shared__ Weights W;
   __shared__ __align__(8) unsigned long long tbar[3];  // bulk-copy completion, one per buffer
-  constexpr int NB = TMA ? Geo::NBUF : 2;
-  double* const buf2 = T2 + Geo::T2VOL + (Geo::PTS ? 3 * NFIELD * NTHREADS : 0);  // TMA with NBUF 3 only
+  // per-thread staging: the next field's copies are issued after the
+  // field-start barrier, which then also frees the previous field's buffer and
+  // T1/T2, so the field step needs no closing barrier
+  constexpr int NB = Geo::NBUF;
+  constexpr bool NEWPIPE = !TMA;
+  double* const buf2 = T2 + Geo::T2VOL + (Geo::PTS ? 3 * NFIELD * NTHREADS : 0);  // used when NBUF is 3
   auto bufp = [&](int b) -> double* { return b == 0 ? buf0 : (b == 1 ? buf1 : buf2); };
 
   const int tid = threadIdx.x;
   const bool batched = args.blocks != nullptr;
   const int lz = tid % TZ, ly = (tid / TZ) % TY, lx = tid / (TZ * TY);
   constexpr int ZS = TMA ? Geo::ZS_TMA : 0;  // z shift of the staged rows
+  // padded T rows only where their extra columns stay inside a staged row
+  constexpr int TROW = Geo::TROW - 4 + R + ZS <= Geo::HZP - 1 ? Geo::TROW : TZ + 6;
+  constexpr int T1N = TX * Geo::T1Y * TROW, T2N = TX * TY * TROW;
   const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R + ZS);
   constexpr int st[3] = {Geo::SX, Geo::SY, 1};
   unsigned tphase = 0;    // bit b: parity of the next completion of tbar[b]
@@ -457,7 +470,8 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       lt = tile - bk.tile0;
       P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
       if (lo != cur_block) {
-        // every thread finished the previous tile's last field step (it ends in a barrier)
+        // every thread must be done with the previous tile's last field step
+        if (NEWPIPE) __syncthreads();
         if (tid < 3) init_weights_h<R>(W, bk.h[tid], args.ko_sigma, tid);
         cur_block = lo;
       }
@@ -535,6 +549,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
     };
     if (TMA) {
       for (int q = 0; q < NB - 1; ++q) tma_issue(stream_field(q), q);
+    } else if (NEWPIPE) {
+      for (int q = 0; q < NB - 1; ++q) {
+        stage_tile<R, T, ZS>(bufp(q), Fbase + (long long)stream_field(q) * n, x0, y0, z0, Sx, Sy, Sz, tid);
+        cp_async_commit();
+      }
     } else {
       stage_tile<R, T, ZS>(buf0, Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
       cp_async_commit();
@@ -555,6 +574,15 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
           clamp_box(bufp(b));
           fence_proxy_async();  // these writes before the next bulk copy into the buffer
           __syncthreads();
+        }
+      } else if (NEWPIPE) {
+        constexpr int PEND = NB - 2 < NFIELD - 1 - idx ? NB - 2 : NFIELD - 1 - idx;  // fields issued after idx
+        cp_async_wait<PEND>();
+        __syncthreads();
+        if (idx + NB - 1 < NFIELD) {
+          stage_tile<R, T, ZS>(bufp((idx + NB - 1) % NB), Fbase + (long long)stream_field(idx + NB - 1) * n, x0,
+                               y0, z0, Sx, Sy, Sz, tid);
+          cp_async_commit();
         }
       } else {
         if (idx + 1 < NFIELD) {
@@ -595,10 +623,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       }
       if (has_d2(f)) {
         // T1 = d/dx over x in [0,TX), y in [-3, TY+3), z in [-3, TZ+3)
-        for (int e = tid; e < Geo::T1N; e += NTHREADS) {
-          const int zz = e % (TZ + 6);
-          const int yy = (e / (TZ + 6)) % Geo::T1Y;
-          const int xx = e / ((TZ + 6) * Geo::T1Y);
+        for (int e = tid; e < T1N; e += NTHREADS) {
+          const int zz = e % TROW;
+          const int yy = (e / TROW) % Geo::T1Y;
+          const int xx = e / (TROW * Geo::T1Y);
           const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R + ZS);
           double s = 0.0;
 #pragma unroll
@@ -607,10 +635,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
           T1[(xx * Geo::T1Y + yy) * HZP + zz] = s;
         }
         // T2 = d/dy over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
-        for (int e = tid; e < Geo::T2N; e += NTHREADS) {
-          const int zz = e % (TZ + 6);
-          const int yy = (e / (TZ + 6)) % TY;
-          const int xx = e / ((TZ + 6) * TY);
+        for (int e = tid; e < T2N; e += NTHREADS) {
+          const int zz = e % TROW;
+          const int yy = (e / TROW) % TY;
+          const int xx = e / (TROW * TY);
           const int cc = (xx + R) * Geo::SX + (yy + R) * Geo::SY + (zz - 3 + R + ZS);
           double s = 0.0;
 #pragma unroll
@@ -637,7 +665,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         for (int p = 0; p < 6; ++p) d2[p] = 0.0;
       }
       acc.consume(f, d1, d2, ko, P, fld);
-      __syncthreads();  // staged buffer and T1/T2 are reused
+      if (!NEWPIPE) __syncthreads();  // staged buffer and T1/T2 are reused
     });
 
     // ---- epilogue ---------------------------------------------------------
@@ -973,12 +1001,12 @@ bool tma_staging_requested() {
 template <int R, int MODE, class T = bssn::DefaultShape>
 int launch_stream(const bssn::Args& a, cudaStream_t stream, int grid) {
   using Geo = bssn::TileGeom<R, T>;
-  const size_t smem = Geo::SMEM + Geo::SMEM_PTS;
+  const size_t smem = Geo::SMEM_RUN;
   CUtensorMap map;
   std::memset(&map, 0, sizeof(map));
   if constexpr (std::is_same<T, bssn::DefaultShape>::value) {
     if (!a.blocks && tma_staging_requested() && make_state_map<R, T>(&map, a.F, a.Sx, a.Sy, a.Sz)) {
-      const size_t smem_tma = Geo::SMEM_TMA;
+      const size_t smem_tma = Geo::SMEM_RUN;
       auto kern = bssn::stream_kernel<R, MODE, T, true>;
       static int flags[kMaxDev] = {0};
       int rc = set_smem(kern, smem_tma, flags);
