@@ -68,6 +68,7 @@ def parse():
                     help="after timing, evolve this many more steps and record the constraint norms")
     ap.add_argument("--track-every", type=int, default=10)
     ap.add_argument("--ozaki-k", type=int, default=0, help="ozaki192: one digit count instead of k = 5..8")
+    ap.add_argument("--ozaki-n", type=int, default=192, help="ozaki192: interior points per axis")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
@@ -556,7 +557,7 @@ def bench_ozaki(args):
     from bssn3d_b200 import initial_data as ID
     from bssn3d_b200.fused_rhs import device_scalars, pack_S, rhs_tensor
     from bssn3d_b200.ozaki import OzakiDerivatives
-    grid, U_host, dt = ID.workload(2)
+    grid, U_host, dt = ID.workload(2, n=args.ozaki_n)
     U = torch.from_numpy(U_host).to(dev)
     S = device_scalars(pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0),
                               grid.dy, grid.dz), dev)
@@ -602,7 +603,7 @@ def bench_ozaki(args):
         "warmup": args.warmup, "ms_per_step": sweep[str(k)]["ms_per_rhs"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "i8 digits, i32 accumulation, f64 algebra",
         "data": "synthetic",
-        "config": {"workload": "Brill-Lindquist q=1/10, 192^3 interior +3 ghosts on [-8,8]^3, one RHS",
+        "config": {"workload": f"Brill-Lindquist q=1/10, {args.ozaki_n}^3 interior +3 ghosts on [-8,8]^3, one RHS",
                    "array": list(grid.shape), "k_chosen_for_1e-10": chosen},
         "fp64_fused": {"ms_per_rhs": fp64_ms, "mpoint_updates_per_s": interior / (fp64_ms * 1e-3) / 1e6},
         "sweep": sweep, "roofline": None, "e2e": None, "cpu_baseline": None,

@@ -9,7 +9,7 @@
 // tensor-core contraction, and the digit results are recombined in float64.
 // The contraction is exact and the recombination order is fixed, so results
 // are bit-reproducible run to run; the only approximation is the split
-// (|residual| <= 2^(e-7k-1) per value).
+// (|residual| <= 2^(e-7k-1) per value, e the window's exponent).
 //
 // This follows the banded-integer-stencil design of the reference's MCS
 // Ozaki derivative (2D/src/mcs2d/schemes/ozaki.py:286-323: stencil matrix,
@@ -18,13 +18,16 @@
 // reference has no Ozaki path for BSSN.
 //
 // Layout of one pass (one field, one axis): the lines of the array along the
-// axis are the rows (M) of the product, the padded positions along the line
-// are K, and the 16 outputs of a tile times 4 stencils (C1, C2 high digit,
-// C2 low digit, KO) are N = 64. A tile is 128 lines x 16 outputs; its K window
-// is 32 padded positions (16 outputs + up to 2x4 halo), one tcgen05.mma
+// axis are the rows (M) of the product, the positions along the line are K,
+// and the 16 outputs of a tile times 4 stencils (C1, C2 high digit, C2 low
+// digit, KO) are N = 64. A tile is 128 lines x 16 outputs; its K window is 32
+// positions (16 outputs + up to 2x4 halo, the rest zero), one tcgen05.mma
 // (M=128, N=64, K=32, kind::i8) per digit plane into its own 64 TMEM columns.
 // Operands sit in shared memory in the canonical no-swizzle K-major layout
 // (8-row x 16-byte core matrices); the banded B matrix is built once per CTA.
+// The exponent is shared by the window of one line in one tile (the
+// reference shares one per block, ozaki.py:316-323); the digit planes are
+// made in shared memory from the float64 window and never touch HBM.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -39,7 +42,6 @@ constexpr int LT = 128;           // lines per tile (MMA M)
 constexpr int NO = 16;            // outputs per tile along the axis
 constexpr int KW = 32;            // K window in padded positions
 constexpr int NCOL = 4 * NO;      // MMA N: C1 | C2 hi | C2 lo | KO
-constexpr int THREADS = 128;      // one thread per line of the tile
 constexpr long long WAIT_LIMIT = 1LL << 26;  // bounded mbarrier polls (~1 s)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -82,114 +84,84 @@ __device__ __forceinline__ long long line_base(int axis, long long l, long long 
   return l * Sz;                                             // l = x*Sy + y
 }
 
-// Padded line length: >= len + 2*4 and a multiple of 16, plus one spare
-// 16-position chunk so that every tile's 32-position window is in range.
-__host__ __device__ constexpr int padded_len(int len) { return ((len + 15) / 16 + 1) * 16; }
+// ---- fused split + contraction + recombination -----------------------------
+// One CTA (256 threads) per SM walks tiles of 128 lines x 16 outputs of one
+// pass. Per tile: the float64 window of each line (16 outputs + 2R halo,
+// edge-clamped) lands in shared memory by cp.async, laid out so that the
+// copies are coalesced (line-contiguous windows for the z axis, line-
+// interleaved for x and y); each line gets one power-of-two exponent for its
+// window and two threads per line write its k digit planes straight into the
+// canonical operand layout; thread 0 issues the k contractions; the two
+// warpgroups read 8 outputs each back from TMEM and recombine them
+// smallest digit first; the outputs go out through shared memory so that the
+// stores are coalesced as well. The next tile's window is prefetched while a
+// tile is contracted.
+constexpr int FT = 256;       // threads of the fused kernel
+constexpr int FW = 33;        // float64 window pitch (conflict-free rows)
+constexpr int OP = 17;        // output staging pitch
 
-// ---- split: one thread per line ------------------------------------------
-__global__ void split_kernel(const double* __restrict__ f, int axis, long long Sx, long long Sy, long long Sz,
-                             int R, int k, int8_t* __restrict__ Q, double* __restrict__ scale) {
-  const Line L = line_geom(axis, Sx, Sy, Sz);
-  const int Lp = padded_len(L.len);
-  for (long long l = blockIdx.x * (long long)blockDim.x + threadIdx.x; l < L.nlines;
-       l += (long long)gridDim.x * blockDim.x) {
-    const double* p = f + line_base(axis, l, Sy, Sz);
-    double m = 0.0;
-    for (int i = 0; i < L.len; ++i) m = fmax(m, fabs(p[(long long)i * L.stride]));
-    int e = 0;
-    if (m > 0.0) {
-      int ex;
-      frexp(m, &ex);  // m = fr * 2^ex, fr in [0.5, 1)
-      e = ex + 1;     // |f| 2^-e < 1/2
-    }
-    scale[l] = ldexp(1.0, e);
-    for (int c = 0; c < Lp / 16; ++c) {
-      uint32_t w[MAXK][4];
-#pragma unroll
-      for (int s = 0; s < MAXK; ++s) w[s][0] = w[s][1] = w[s][2] = w[s][3] = 0u;
-#pragma unroll
-      for (int i = 0; i < 16; ++i) {
-        const int zp = 16 * c + i;
-        double v = 0.0;
-        if (zp < L.len + 2 * R) {
-          int q = zp - R;
-          q = q < 0 ? 0 : (q > L.len - 1 ? L.len - 1 : q);  // edge padding (derivatives.py:83-84)
-          v = p[(long long)q * L.stride];
-        }
-        double r = ldexp(v, -e);
-#pragma unroll
-        for (int s = 0; s < MAXK; ++s) {
-          if (s < k) {
-            const double t = r * 128.0;
-            const double d = rint(t);
-            r = t - d;
-            const uint32_t byte = (uint32_t)(uint8_t)(int8_t)(int)d;
-            w[s][i >> 2] |= byte << (8 * (i & 3));
-          }
-        }
-      }
-#pragma unroll
-      for (int s = 0; s < MAXK; ++s) {
-        if (s < k) {
-          uint4* dst = reinterpret_cast<uint4*>(Q + ((long long)s * L.nlines + l) * Lp + 16 * c);
-          *dst = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
-        }
-      }
-    }
-  }
-}
-
-// ---- contraction + recombination -------------------------------------------
-struct MmaArgs {
-  const int8_t* Q;
-  const double* scale;
+struct FusedArgs {
+  const double* src;
   int axis;
   long long Sx, Sy, Sz;
-  int R;        // padding reach of the split (3, or 4 with KO8)
-  int k;        // digits
-  int ko_reach; // 3 (KO6) or 4 (KO8)
-  const double* S;  // scalar pack (device); the spacing of `axis` is S[13 + axis]
+  int R, k, ko_reach;
+  const double* S;
   double ko_sigma;
-  double* d1;   // first derivative out (or NULL)
-  double* d2;   // diagonal second derivative out (or NULL)
-  double* ko;   // KO term out (or NULL)
-  int ko_add;   // add to *ko instead of storing
-  int* err;     // set to 1 if a tensor-core wait gives up
+  double* d1;
+  double* d2;
+  double* ko;
+  int ko_add;
+  int* err;
 };
 
-__global__ void __launch_bounds__(THREADS, 1) mma_kernel(const MmaArgs a) {
-  __shared__ __align__(128) int8_t sB[NCOL * KW];
-  __shared__ __align__(128) int8_t sA[MAXK][LT * KW];
+struct FusedSmem {
+  int8_t B[NCOL * KW];
+  int8_t A[MAXK][LT * KW];
+  double F[2][LT * FW];
+  double O[3][LT * OP];
+  long long base[2][LT];  // first element of each line of the tile in F[buf]
+};
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+
+template <int R, int AXIS>
+__global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
+  extern __shared__ __align__(128) unsigned char fsm_raw[];
+  FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fsm_raw);
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5;
-  const Line L = line_geom(a.axis, a.Sx, a.Sy, a.Sz);
-  const int Lp = padded_len(L.len);
-  const double h = a.S[13 + a.axis];
+  if (smem_u32(fsm_raw) & 127u) {  // operand layouts need an aligned base: refuse rather than misplace
+    if (tid == 0) atomicExch(a.err, 1);
+    return;
+  }
+  const Line L = line_geom(AXIS, a.Sx, a.Sy, a.Sz);
+  constexpr int KWL = NO + 2 * R;  // window positions the stencils use (22 or 24)
+  const double h = a.S[13 + AXIS];
   const double w1 = (1.0 / 60.0) * (1.0 / h);
   const double w2 = (1.0 / 180.0) * (1.0 / (h * h));
-  const double wko = (1.0 / (a.ko_reach == 4 ? 256.0 : 64.0)) * (a.ko_sigma / h);
-
-  // banded stencil matrix: row n = stencil*16 + output o, column kb = window position
+  const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / h);
   {
     const int c1[7] = {-1, 9, -45, 0, 45, -9, 1};
     const int c2h[7] = {0, 0, 2, -4, 2, 0, 0};       // 270 = 2*128 + 14, -490 = -4*128 + 22
     const int c2l[7] = {2, -27, 14, 22, 14, -27, 2};
     const int k6[7] = {1, -6, 15, -20, 15, -6, 1};
     const int k8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1};
-    for (int i = tid; i < NCOL * KW; i += THREADS) {
+    for (int i = tid; i < NCOL * KW; i += FT) {
       const int n = i / KW, kb = i % KW;
       const int st = n / NO, o = n % NO;
-      const int j = kb - a.R - o;  // tap offset
+      const int j = kb - R - o;
       int v = 0;
       if (st < 3) {
         if (j >= -3 && j <= 3) v = st == 0 ? c1[j + 3] : (st == 1 ? c2h[j + 3] : c2l[j + 3]);
-      } else if (a.ko_reach == 4) {
+      } else if (R == 4) {
         if (j >= -4 && j <= 4) v = k8[j + 4];
       } else {
         if (j >= -3 && j <= 3) v = k6[j + 3];
       }
-      sB[canon(n, kb, NCOL)] = (int8_t)v;
+      sm.B[canon(n, kb, NCOL)] = (int8_t)v;
     }
   }
   if (tid == 0) {
@@ -209,42 +181,96 @@ __global__ void __launch_bounds__(THREADS, 1) mma_kernel(const MmaArgs a) {
   const long long nlb = (L.nlines + LT - 1) / LT;
   const int nzt = (L.len + NO - 1) / NO;
   const long long ntiles = nlb * nzt;
-  uint32_t phase = 0;
-  bool failed = false;
-  for (long long tile = blockIdx.x; tile < ntiles && !failed; tile += gridDim.x) {
-    const long long lb = tile / nzt;
-    const int zt = (int)(tile % nzt);
-    const int z0 = zt * NO;
-    // ---- stage the digit planes of 128 lines x 32 positions (16-byte cp.async) ----
-    for (int i = tid; i < a.k * LT * 2; i += THREADS) {
-      const int s = i / (LT * 2);
-      const int rem = i % (LT * 2);
-      const int r = rem >> 1, kc = rem & 1;
-      long long l = lb * LT + r;
-      if (l >= L.nlines) l = L.nlines - 1;  // tail rows recompute the last line, results dropped
-      const int8_t* src = a.Q + ((long long)s * L.nlines + l) * Lp + z0 + 16 * kc;
-      const uint32_t dst = smem_u32(&sA[s][canon(r, 16 * kc, LT)]);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+  constexpr bool zaxis = AXIS == 2;
+  // the window of tile t into F[buf] (edge-clamped positions, tail lines repeat
+  // the last line); the lines' first elements are tabled once per tile. Ends
+  // in a barrier-free state: callers place it right after a barrier.
+  auto load_window = [&](long long t, int buf) {
+    const long long lb = t / nzt;
+    const int z0 = (int)(t % nzt) * NO;
+    if (tid < LT) {
+      long long l = lb * LT + tid;
+      if (l >= L.nlines) l = L.nlines - 1;
+      sm.base[buf][tid] = line_base(AXIS, l, a.Sy, a.Sz);
+    }
+    __syncthreads();
+    for (int i = tid; i < LT * KWL; i += FT) {
+      const int r = zaxis ? i / KWL : i % LT;
+      const int pos = zaxis ? i % KWL : i / LT;
+      int q = z0 - R + pos;
+      q = q < 0 ? 0 : (q > L.len - 1 ? L.len - 1 : q);  // edge padding (derivatives.py:83-84)
+      cp_async8(&sm.F[buf][r * FW + pos], a.src + sm.base[buf][r] + (long long)q * L.stride);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
+  };
+  uint32_t phase = 0;
+  bool failed = false;
+  long long tile = blockIdx.x;
+  if (tile < ntiles) load_window(tile, 0);
+  int buf = 0;
+  for (; tile < ntiles && !failed; tile += gridDim.x, buf ^= 1) {
+    const long long lb = tile / nzt;
+    const int z0 = (int)(tile % nzt) * NO;
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+    // ---- exponent and digits: threads r and r + 128 take the two 16-position halves of line r ----
+    const int r = tid & (LT - 1), half = tid >> 7;
+    const double* Fr = &sm.F[buf][r * FW];
+    double m0 = 0.0, m1 = 0.0;
+#pragma unroll
+    for (int pos = 0; pos < KWL; pos += 2) {
+      m0 = fmax(m0, fabs(Fr[pos]));
+      m1 = fmax(m1, fabs(Fr[pos + 1]));
+    }
+    const double m = fmax(m0, m1);
+    int e = 0;
+    if (m > 0.0) {
+      int ex;
+      frexp(m, &ex);  // m = fr * 2^ex, fr in [0.5, 1)
+      e = ex + 1;     // |f| 2^-e < 1/2
+    }
+    const double sc = ldexp(1.0, e);
+    const double isc = ldexp(1.0, -e);  // scaling by a power of two is exact
+    {
+      uint32_t wd[MAXK][4];
+#pragma unroll
+      for (int s2 = 0; s2 < MAXK; ++s2) wd[s2][0] = wd[s2][1] = wd[s2][2] = wd[s2][3] = 0u;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int pos = 16 * half + j;
+        double rr = pos < KWL ? Fr[pos] * isc : 0.0;
+#pragma unroll
+        for (int s2 = 0; s2 < MAXK; ++s2) {
+          if (s2 < a.k) {
+            const double t = rr * 128.0;
+            const double d = rint(t);
+            rr = t - d;
+            wd[s2][j >> 2] |= (uint32_t)(uint8_t)(int8_t)(int)d << (8 * (j & 3));
+          }
+        }
+      }
+#pragma unroll
+      for (int s2 = 0; s2 < MAXK; ++s2)
+        if (s2 < a.k)
+          *reinterpret_cast<uint4*>(&sm.A[s2][canon(r, 16 * half, LT)]) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
+    }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
-    // ---- one elected thread issues the k contractions and commits them ----
+    // ---- prefetch the next tile's window; thread 0 issues the contractions ----
+    if (tile + gridDim.x < ntiles) load_window(tile + gridDim.x, buf ^ 1);
     if (tid == 0) {
-      const uint64_t db = smem_desc(smem_u32(sB), NCOL * 16, 128);
-      for (int s = 0; s < a.k; ++s) {
-        const uint64_t da = smem_desc(smem_u32(&sA[s][0]), LT * 16, 128);
+      const uint64_t db = smem_desc(smem_u32(sm.B), NCOL * 16, 128);
+      for (int s2 = 0; s2 < a.k; ++s2) {
+        const uint64_t da = smem_desc(smem_u32(&sm.A[s2][0]), LT * 16, 128);
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NCOL * s)),
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NCOL * s2)),
             "l"(da), "l"(db), "r"(IDESC), "r"(0u));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                        smem_u32(&mbar))
                    : "memory");
     }
-    // ---- bounded wait for the contractions ----
     uint32_t done = 0;
     for (long long it = 0; it < WAIT_LIMIT && !done; ++it) {
       asm volatile(
@@ -253,63 +279,62 @@ __global__ void __launch_bounds__(THREADS, 1) mma_kernel(const MmaArgs a) {
           : "r"(smem_u32(&mbar)), "r"(phase)
           : "memory");
     }
-    if (__syncthreads_or(!done)) {  // one uniform verdict for the whole CTA
+    if (__syncthreads_or(!done)) {
       if (tid == 0) atomicExch(a.err, 1);
       failed = true;
     }
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // ---- recombine in float64: thread = line (TMEM lane) ----
-    const long long l = lb * LT + tid;
-    const bool line_ok = l < L.nlines && !failed;
-    const double sc = line_ok ? a.scale[l] : 0.0;
-    const long long base = line_ok ? line_base(a.axis, l, a.Sy, a.Sz) : 0;
-    const uint32_t lane = (uint32_t)(warp * 32) << 16;
-    double r1[NO], r2[NO], rk[NO];
+    // ---- recombine: warp w reads TMEM lanes 32 (w % 4).., outputs 8 (w / 4).. ----
+    const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
+    const int oc = 8 * (warp >> 2);
+    double r1[8], r2[8], rk[8];
 #pragma unroll
-    for (int o = 0; o < NO; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
-    for (int s = a.k - 1; s >= 0; --s) {
-      uint32_t v[4][NO];
+    for (int o = 0; o < 8; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
+    double w = ldexp(1.0, -7 * a.k);  // weight of the smallest digit plane
+    for (int s2 = a.k - 1; s2 >= 0; --s2, w *= 128.0) {
+      uint32_t v[4][8];
 #pragma unroll
       for (int st = 0; st < 4; ++st) {
-        const uint32_t addr = tmem + lane + (uint32_t)(NCOL * s + NO * st);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-            : "=r"(v[st][0]), "=r"(v[st][1]), "=r"(v[st][2]), "=r"(v[st][3]), "=r"(v[st][4]), "=r"(v[st][5]),
-              "=r"(v[st][6]), "=r"(v[st][7]), "=r"(v[st][8]), "=r"(v[st][9]), "=r"(v[st][10]), "=r"(v[st][11]),
-              "=r"(v[st][12]), "=r"(v[st][13]), "=r"(v[st][14]), "=r"(v[st][15])
-            : "r"(addr));
+        const uint32_t addr = tmem + lane + (uint32_t)(NCOL * s2 + NO * st + oc);
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                     : "=r"(v[st][0]), "=r"(v[st][1]), "=r"(v[st][2]), "=r"(v[st][3]), "=r"(v[st][4]),
+                       "=r"(v[st][5]), "=r"(v[st][6]), "=r"(v[st][7])
+                     : "r"(addr));
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      const double w = ldexp(1.0, -7 * (s + 1));
 #pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        const int i1 = (int)v[0][o];
-        const int i2 = (int)v[1][o] * 128 + (int)v[2][o];
-        const int ik = (int)v[3][o];
-        r1[o] += (double)i1 * w;
-        r2[o] += (double)i2 * w;
-        rk[o] += (double)ik * w;
+      for (int o = 0; o < 8; ++o) {
+        r1[o] += (double)(int)v[0][o] * w;
+        r2[o] += (double)((int)v[1][o] * 128 + (int)v[2][o]) * w;
+        rk[o] += (double)(int)v[3][o] * w;
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    if (line_ok) {
+    // the recombining thread's line is r too (TMEM lane = line): its exponent is sc
 #pragma unroll
-      for (int o = 0; o < NO; ++o) {
-        const int z = z0 + o;
-        if (z < L.len) {
-          const long long pt = base + (long long)z * L.stride;
-          if (a.d1) a.d1[pt] = (r1[o] * sc) * w1;
-          if (a.d2) a.d2[pt] = (r2[o] * sc) * w2;
-          if (a.ko) {
-            const double kv = (rk[o] * sc) * wko;
-            a.ko[pt] = a.ko_add ? a.ko[pt] + kv : kv;
-          }
-        }
+    for (int o = 0; o < 8; ++o) {
+      sm.O[0][r * OP + oc + o] = (r1[o] * sc) * w1;
+      sm.O[1][r * OP + oc + o] = (r2[o] * sc) * w2;
+      sm.O[2][r * OP + oc + o] = (rk[o] * sc) * wko;
+    }
+    __syncthreads();
+    // ---- coalesced stores of the tile's outputs ----
+    for (int i = tid; i < LT * NO; i += FT) {
+      const int rr = zaxis ? i / NO : i % LT;
+      const int o = zaxis ? i % NO : i / LT;
+      const long long l = lb * LT + rr;
+      const int z = z0 + o;
+      if (l < L.nlines && z < L.len && !failed) {
+        const long long pt = sm.base[buf][rr] + (long long)z * L.stride;
+        if (a.d1) a.d1[pt] = sm.O[0][rr * OP + o];
+        if (a.d2) a.d2[pt] = sm.O[1][rr * OP + o];
+        if (a.ko) a.ko[pt] = a.ko_add ? a.ko[pt] + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
       }
     }
-    __syncthreads();  // TMEM columns and shared operands are reused by the next tile
+    __syncthreads();  // TMEM columns, digits and output staging are reused by the next tile
   }
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
@@ -320,6 +345,19 @@ __global__ void __launch_bounds__(THREADS, 1) mma_kernel(const MmaArgs a) {
 // ======================================================================
 namespace {
 thread_local std::string g_oz_err;
+
+template <int R, int AXIS>
+cudaError_t launch_fused(const ozaki::FusedArgs& m, int grid, cudaStream_t st, int dev) {
+  static bool attr_done[64] = {false};
+  constexpr int kSmem = (int)sizeof(ozaki::FusedSmem);
+  if (!attr_done[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (e != cudaSuccess) return e;
+    attr_done[dev] = true;
+  }
+  ozaki::fused_kernel<R, AXIS><<<grid, ozaki::FT, kSmem, st>>>(m);
+  return cudaSuccess;
+}
 int oz_fail(int code, const std::string& m) {
   g_oz_err = m;
   return code;
@@ -332,15 +370,7 @@ const char* bssn_b200_ozaki_last_error(void) { return g_oz_err.c_str(); }
 
 size_t bssn_b200_ozaki_workspace_bytes(long long Sx, long long Sy, long long Sz, int k) {
   if (Sx < 1 || Sy < 1 || Sz < 1 || k < 1 || k > ozaki::MAXK) return 0;
-  size_t best = 0;
-  for (int axis = 0; axis < 3; ++axis) {
-    const ozaki::Line L = ozaki::line_geom(axis, Sx, Sy, Sz);
-    const size_t q = (size_t)k * (size_t)L.nlines * (size_t)ozaki::padded_len(L.len);
-    const size_t sc = (size_t)L.nlines * sizeof(double);
-    const size_t need = ((q + 255) / 256) * 256 + sc;
-    if (need > best) best = need;
-  }
-  return best + 256;  // + the error flag
+  return 256;  // the error flag (the digit planes never leave shared memory)
 }
 
 int* bssn_b200_ozaki_error_flag(void* workspace, long long Sx, long long Sy, long long Sz, int k) {
@@ -366,15 +396,8 @@ int bssn_b200_ozaki_derivatives(void* stream, const double* F, const double* S, 
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
-  // One CTA per SM: the contraction kernel owns all 512 TMEM columns.
-  static bool attr_done[64] = {false};
-  constexpr int kPadSmem = 120 * 1024;
-  if (dev >= 0 && dev < 64 && !attr_done[dev]) {
-    e = cudaFuncSetAttribute(ozaki::mma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kPadSmem);
-    if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
-    attr_done[dev] = true;
-  }
-  char* ws = static_cast<char*>(workspace);
+  // One CTA per SM: the fused kernel owns all 512 TMEM columns.
+  if (dev < 0 || dev >= 64) return oz_fail(BSSN_B200_EINVAL, "ozaki: device ordinal out of range");
   int* err = bssn_b200_ozaki_error_flag(workspace, Sx, Sy, Sz, k);
   e = cudaMemsetAsync(err, 0, sizeof(int), st);
   if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
@@ -382,19 +405,20 @@ int bssn_b200_ozaki_derivatives(void* stream, const double* F, const double* S, 
   const int R = (use_ko && ko_order == 8) ? 4 : 3;
   auto pass = [&](const double* src, int axis, double* d1, double* d2, double* ko, int ko_add) -> int {
     const ozaki::Line L = ozaki::line_geom(axis, Sx, Sy, Sz);
-    const size_t qbytes = (size_t)k * (size_t)L.nlines * (size_t)ozaki::padded_len(L.len);
-    int8_t* Q = reinterpret_cast<int8_t*>(ws);
-    double* scale = reinterpret_cast<double*>(ws + ((qbytes + 255) / 256) * 256);
-    const int sblocks = (int)((L.nlines + 127) / 128);
-    ozaki::split_kernel<<<sblocks, 128, 0, st>>>(src, axis, Sx, Sy, Sz, R, k, Q, scale);
-    ozaki::MmaArgs m{};
-    m.Q = Q; m.scale = scale; m.axis = axis; m.Sx = Sx; m.Sy = Sy; m.Sz = Sz;
+    ozaki::FusedArgs m{};
+    m.src = src; m.axis = axis; m.Sx = Sx; m.Sy = Sy; m.Sz = Sz;
     m.R = R; m.k = k; m.ko_reach = R; m.S = S; m.ko_sigma = use_ko ? ko_sigma : 0.0;
     m.d1 = d1; m.d2 = d2; m.ko = ko; m.ko_add = ko_add; m.err = err;
     const long long tiles = ((L.nlines + ozaki::LT - 1) / ozaki::LT) * ((L.len + ozaki::NO - 1) / ozaki::NO);
     const int grid = (int)(tiles < sms ? tiles : sms);
-    ozaki::mma_kernel<<<grid, ozaki::THREADS, kPadSmem, st>>>(m);
-    cudaError_t le = cudaGetLastError();
+    cudaError_t le;
+    if (R == 4)
+      le = axis == 0 ? launch_fused<4, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<4, 1>(m, grid, st, dev)
+                                                                        : launch_fused<4, 2>(m, grid, st, dev));
+    else
+      le = axis == 0 ? launch_fused<3, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<3, 1>(m, grid, st, dev)
+                                                                        : launch_fused<3, 2>(m, grid, st, dev));
+    if (le == cudaSuccess) le = cudaGetLastError();
     if (le != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki launch: ") + cudaGetErrorString(le));
     return 0;
   };
