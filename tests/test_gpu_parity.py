@@ -279,3 +279,31 @@ def test_constraint_norms_fused_vs_oracle_and_reproducible():
     h, m = O.constraint_norms(U, grid.dx, grid.dy, grid.dz, grid.ng)
     assert a[0] == pytest.approx(h, rel=1e-12)
     assert a[1] == pytest.approx(m, rel=1e-12, abs=1e-300)
+
+
+def _reference_vector_recipe(npts=1 << 18, seed=1):
+    """Inputs of the reference's algebra-only vector file
+    (3D/src/bssn3d/cuda/gen_algebra_cuda.py:99-140): near-Minkowski fields
+    (1 or 0 plus 0.03 N(0,1), drawn in state order), derivatives 0.03 N(0,1),
+    default physics, dt 0.01, dx 0.1, t 0."""
+    rng = np.random.default_rng(seed)
+    F = np.empty((24, npts))
+    for f in range(24):
+        F[f] = (1.0 if f in (0, 1, 3, 6, 8) else 0.0) + 0.03 * rng.standard_normal(npts)
+    D = 0.03 * rng.standard_normal((138, npts))
+    S = _S(0.1, 0.1, 0.1, dt=0.01, t=0.0)
+    return F, D, S
+
+
+def test_algebra_reference_vector_recipe():
+    F, D, S = _reference_vector_recipe()
+    Fd, Dd, Sd = _dev(F), _dev(D), _dev(S)
+    out = torch.empty_like(Fd)
+    L = _lib()
+    L.check(L.load().bssn_b200_rhs_algebra(None, Fd.data_ptr(), Dd.data_ptr(), Sd.data_ptr(), out.data_ptr(),
+                                           F.shape[1]))
+    got = out.cpu().numpy()
+    assert np.isfinite(got).all()
+    assert O.normwise_rel(got, O.rhs_algebra(F, D, S)).max() < 1e-12
+    if O.have_ref():
+        assert O.normwise_rel(got, O.ref_rhs_algebra(F, D, S)).max() < 1e-12

@@ -171,3 +171,18 @@ def test_constraints_vs_compiled_physcon():
     Hr, Mr = O.ref_constraints_algebra(F, D)
     assert np.abs(H - Hr).max() <= 1e-13 * np.abs(Hr).max()
     assert np.abs(M - Mr).max() <= 1e-13 * np.abs(Mr).max()
+
+
+def test_oracle_algebra_on_the_reference_vector_recipe():
+    """The oracle against the reference's compiled algebra on the inputs of its
+    algebra-only vector file (gen_algebra_cuda.py:99-140), 2^16 of its 2^18 points."""
+    if not O.have_ref():
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(1)
+    n = 1 << 16
+    F = np.empty((24, n))
+    for f in range(24):
+        F[f] = (1.0 if f in (0, 1, 3, 6, 8) else 0.0) + 0.03 * rng.standard_normal(n)
+    D = 0.03 * rng.standard_normal((138, n))
+    S = np.array([2.0, 0.06, 0.01, 0.1, 0.6, 20.0, 0.0, 1, 1, 1, 1, 1, 0, 0.1, 0.1, 0.1])
+    assert O.normwise_rel(O.rhs_algebra(F, D, S), O.ref_rhs_algebra(F, D, S)).max() < 1e-13
