@@ -245,6 +245,9 @@ __device__ __forceinline__ void stage_tile(double* buf, const double* __restrict
                                            long long y0, long long z0, long long Sx, long long Sy,
                                            long long Sz, int tid) {
   using Geo = TileGeom<R, T>;
+  // 32-bit index arithmetic: a grid holds fewer than 2^31 points (check_grid)
+  const int bx = (int)x0 - R, by = (int)y0 - R, bz = (int)z0 - R;
+  const int mx = (int)Sx - 1, my = (int)Sy - 1, mz = (int)Sz - 1, sy = (int)Sy, sz = (int)Sz;
 #pragma unroll
   for (int e = 0; e < Geo::PER_THREAD; ++e) {
     const int idx = tid + e * NTHREADS;
@@ -252,10 +255,10 @@ __device__ __forceinline__ void stage_tile(double* buf, const double* __restrict
       const int hz = idx % Geo::HZ;
       const int hy = (idx / Geo::HZ) % Geo::HY;
       const int hx = idx / (Geo::HZ * Geo::HY);
-      const long long qx = clampll(x0 - R + hx, Sx - 1);
-      const long long qy = clampll(y0 - R + hy, Sy - 1);
-      const long long qz = clampll(z0 - R + hz, Sz - 1);
-      cp_async8(buf + hx * Geo::SX + hy * Geo::SY + hz + ZS, Ff + (qx * Sy + qy) * Sz + qz);
+      const int qx = min(max(bx + hx, 0), mx);
+      const int qy = min(max(by + hy, 0), my);
+      const int qz = min(max(bz + hz, 0), mz);
+      cp_async8(buf + hx * Geo::SX + hy * Geo::SY + hz + ZS, Ff + ((qx * sy + qy) * sz + qz));
     }
   }
 }
@@ -1125,6 +1128,10 @@ int bssn_b200_batch_plan(bssn_b200_block* host_blocks, int nblocks, int variant)
     bssn_b200_block& bk = host_blocks[b];
     if (bk.sx < 1 || bk.sy < 1 || bk.sz < 1 || bk.offset < 0 || !(bk.h[0] > 0) || !(bk.h[1] > 0) || !(bk.h[2] > 0)) {
       fail(BSSN_B200_EINVAL, "batch_plan: block " + std::to_string(b) + " has a bad extent, offset or spacing");
+      return -1;
+    }
+    if ((long long)bk.sx * bk.sy * bk.sz >= (1LL << 31)) {
+      fail(BSSN_B200_EINVAL, "batch_plan: block " + std::to_string(b) + " has 2^31 points or more");
       return -1;
     }
     if (bk.core < 0 || 2 * bk.core >= bk.sx || 2 * bk.core >= bk.sy || 2 * bk.core >= bk.sz) {
