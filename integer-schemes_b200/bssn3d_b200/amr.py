@@ -138,15 +138,18 @@ class BlockPool:
         self.tile = tuple(tile)
         self.table, self.ntiles = self.descriptors(self.tile)
 
-    def descriptors(self, tile, core: bool = False):
+    def descriptors(self, tile, core: bool = False, active=None):
         """Block table and tile count; ``core=True`` leaves each block's ghost
-        layers out of the tiles (they come from a ghost fill)."""
+        layers out of the tiles (they come from a ghost fill); ``active``
+        (block indices) limits the table to the blocks a launch evolves."""
         TX, TY, TZ = tile
-        arr = (BlockDesc * len(self.blocks))()
+        idx = list(range(len(self.blocks))) if active is None else list(active)
+        arr = (BlockDesc * len(idx))()
         t0 = 0
-        for i, b in enumerate(self.blocks):
+        for j, i in enumerate(idx):
+            b = self.blocks[i]
             sx, sy, sz = b.shape
-            d = arr[i]
+            d = arr[j]
             d.offset = int(self.offsets[i])
             d.sx, d.sy, d.sz = sx, sy, sz
             d.tile0 = t0
@@ -196,7 +199,8 @@ class BatchedEvolution:
     """
 
     def __init__(self, pool: BlockPool, params=None, ko_sigma: float = 0.1, ko_order: int = 6,
-                 variant: int = 0, device="cuda", ghosts: str = "evolve", restrict: bool = False):
+                 variant: int = 0, device="cuda", ghosts: str = "evolve", restrict: bool = False,
+                 plan=None, active=None):
         import torch
         from .state import PhysicsParams
         from . import _lib
@@ -206,6 +210,8 @@ class BatchedEvolution:
             raise ValueError("restrict needs ghosts='exchange'")
         self.ghosts = ghosts
         self.pool = pool
+        # blocks the stage kernels evolve (all, unless a rank holds mirrors of remote blocks)
+        self.active = list(range(len(pool.blocks))) if active is None else list(active)
         self.params = params or PhysicsParams()
         self.ko_sigma = float(ko_sigma)
         self.ko_order = int(ko_order)
@@ -218,7 +224,7 @@ class BatchedEvolution:
         self.dplan = None
         if ghosts == "exchange":
             from .ghosts import DevicePlan, GhostPlan
-            self.plan = GhostPlan(pool, restrict=restrict)
+            self.plan = plan if plan is not None else GhostPlan(pool, restrict=restrict)
             self.dplan = DevicePlan(self.plan, self.device)
         self.set_variant(variant)
         self._bufs = None
@@ -226,8 +232,8 @@ class BatchedEvolution:
     def set_variant(self, variant: int) -> None:
         import torch
         lib = self._lib.load()
-        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange")
-        ntiles = lib.bssn_b200_batch_plan(ctypes.addressof(table), len(self.pool.blocks), int(variant))
+        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange", active=self.active)
+        ntiles = lib.bssn_b200_batch_plan(ctypes.addressof(table), len(self.active), int(variant))
         if ntiles < 0:
             self._lib.check(self._lib.EINVAL)
         raw = bytes(memoryview(table).cast("B"))
@@ -276,7 +282,7 @@ class BatchedEvolution:
         rc = lib.bssn_b200_batch_rk4_stage(self._stream(), stage, U.data_ptr(), Y.data_ptr(), ACC.data_ptr(),
                                            YNEXT.data_ptr(), S.data_ptr(), self.ko_sigma, self.ko_order,
                                            p.chi_floor, p.alpha_floor, self.table_dev.data_ptr(),
-                                           len(self.pool.blocks), self.ntiles, self.variant)
+                                           len(self.active), self.ntiles, self.variant)
         self._lib.check(rc)
 
     def rhs(self, U, S):
@@ -291,7 +297,7 @@ class BatchedEvolution:
         else:
             out = torch.empty_like(U)
         rc = self._lib.load().bssn_b200_batch_rhs(self._stream(), U.data_ptr(), S.data_ptr(), out.data_ptr(),
-                                                  self.table_dev.data_ptr(), len(self.pool.blocks),
+                                                  self.table_dev.data_ptr(), len(self.active),
                                                   self.ntiles, self.variant)
         self._lib.check(rc)
         return out
@@ -362,32 +368,39 @@ class BatchedEvolution:
                                              p.chi_floor, p.alpha_floor, sx, sy, sz)
                 self._lib.check(rc)
 
-    def constraint_norms(self, U):
-        """Interior L2 norms (H, |M|) over every block's interior points
-        together: each block's norms come from the fused norm kernel
-        (constraints.py:53-62 per block) and are combined weighted by the
-        block's interior point count. With ghost exchange a filled copy of U
-        is measured."""
+    def constraint_sums(self, U, filled: bool = False):
+        """Device tensor (sum of H^2, sum of |M|^2, point count) over the
+        interior points of the blocks this object evolves: each block's norms
+        come from the fused norm kernel (constraints.py:53-62 per block) and
+        are weighted by its interior point count. With ghost exchange the
+        ghosts of a copy of U are filled first (unless ``filled``)."""
         import torch
         from .fused_rhs import device_scalars, pack_S
         lib = self._lib.load()
-        if self.ghosts == "exchange":
+        if self.ghosts == "exchange" and not filled:
             U = U.clone()
             self.fill(U)
         need = int(lib.bssn_b200_norms_scratch_bytes())
         scratch = torch.empty(need // 8 + 1, dtype=torch.float64, device=self.device)
-        out = torch.empty(len(self.pool.blocks), 2, dtype=torch.float64, device=self.device)
-        for i, blk in enumerate(self.pool.blocks):
+        out = torch.empty(len(self.active), 2, dtype=torch.float64, device=self.device)
+        for j, i in enumerate(self.active):
+            blk = self.pool.blocks[i]
             S = device_scalars(pack_S(2.0, 0.0, 1.0, blk.h, 0.0, 1.0, 0.0, (1, 1, 1, 1), (1, 0),
                                       blk.h, blk.h), self.device)
             o = int(self.pool.offsets[i])
             sx, sy, sz = blk.shape
             rc = lib.bssn_b200_constraint_norms(self._stream(), U[o:].data_ptr(), S.data_ptr(), sx, sy, sz,
-                                                blk.ng, scratch.data_ptr(), need, out[i].data_ptr())
+                                                blk.ng, scratch.data_ptr(), need, out[j].data_ptr())
             self._lib.check(rc)
-        w = torch.tensor([float(b.interior_points) for b in self.pool.blocks], dtype=torch.float64,
+        w = torch.tensor([float(self.pool.blocks[i].interior_points) for i in self.active], dtype=torch.float64,
                          device=self.device)
-        hm = torch.sqrt((out ** 2 * w[:, None]).sum(0) / w.sum())
+        return torch.cat([(out ** 2 * w[:, None]).sum(0), w.sum().reshape(1)])
+
+    def constraint_norms(self, U):
+        """Interior L2 norms (H, |M|) over every block's interior points together."""
+        import torch
+        sums = self.constraint_sums(U)
+        hm = torch.sqrt(sums[:2] / sums[2])
         return float(hm[0]), float(hm[1])
 
     def block_scalars(self, t: float, dt: float):

@@ -294,8 +294,14 @@ class DevicePlan:
     def run(self, which: str, pool_tensor, stream) -> None:
         """Enqueue the ``"fill"`` (coarse to fine) or ``"restrict"`` (fine to
         coarse) launches on ``pool_tensor``."""
+        for lvl, _, _, _ in getattr(self, which):
+            self.run_level(which, lvl, pool_tensor, stream)
+
+    def run_level(self, which: str, level: int, pool_tensor, stream) -> None:
+        """Enqueue the one launch of ``which`` for ``level`` (if it has ops)."""
         from . import _lib
         lib = _lib.load()
-        for _, dev, nops, npts in getattr(self, which):
-            _lib.check(lib.bssn_b200_fill(stream, pool_tensor.data_ptr(), dev.data_ptr(), nops, npts,
-                                          ctypes.cast(self.wmid, ctypes.c_void_p)))
+        for lvl, dev, nops, npts in getattr(self, which):
+            if lvl == level:
+                _lib.check(lib.bssn_b200_fill(stream, pool_tensor.data_ptr(), dev.data_ptr(), nops, npts,
+                                              ctypes.cast(self.wmid, ctypes.c_void_p)))

@@ -177,7 +177,8 @@ struct TileGeom {
   static constexpr unsigned TMA_BYTES = (unsigned)(BOXZ * HY * HX * sizeof(double));
   static constexpr int SX = HY * HZP, SY = HZP;
   static constexpr int VOL = HX * HY * HZP;   // doubles per staged buffer
-  static constexpr int NELEM = HX * HY * HZ;  // staged elements
+  static constexpr int HZS = HZ;             // staged row length (full 24-wide rows measured 1.5 % slower)
+  static constexpr int NELEM = HX * HY * HZS;  // staged elements
   static constexpr int PER_THREAD = (NELEM + NTHREADS - 1) / NTHREADS;
   // separable mixed-derivative passes
   static constexpr int TP = zpitch(TZ + 6);                       // z pitch of T1/T2
@@ -252,9 +253,9 @@ __device__ __forceinline__ void stage_tile(double* buf, const double* __restrict
   for (int e = 0; e < Geo::PER_THREAD; ++e) {
     const int idx = tid + e * NTHREADS;
     if (idx < Geo::NELEM) {
-      const int hz = idx % Geo::HZ;
-      const int hy = (idx / Geo::HZ) % Geo::HY;
-      const int hx = idx / (Geo::HZ * Geo::HY);
+      const int hz = idx % Geo::HZS;
+      const int hy = (idx / Geo::HZS) % Geo::HY;
+      const int hx = idx / (Geo::HZS * Geo::HY);
       const int qx = min(max(bx + hx, 0), mx);
       const int qy = min(max(by + hy, 0), my);
       const int qz = min(max(bz + hz, 0), mz);

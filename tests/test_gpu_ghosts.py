@@ -219,3 +219,17 @@ def test_workload_exchange_steps_stay_finite_with_constraint_norms():
     h1, m1 = evo.constraint_norms(out)
     assert np.isfinite([h0, m0, h1, m1]).all()
     assert h1 < 10 * h0 + 1.0
+
+
+def test_distributed_evolution_one_rank_equals_batched_exchange():
+    from bssn3d_b200 import amr
+    from bssn3d_b200.parallel import DistributedBatchedEvolution
+    pool, punct = _pool(count=10, seed=7, domain=6.0, sizes=(8, 10, 12))
+    U = torch.from_numpy(pool.initial_state(punct, seed=2)).cuda()
+    dt = 0.25 * min(b.h for b in pool.blocks)
+    ref = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, ghosts="exchange")
+    dist_evo = DistributedBatchedEvolution(pool.blocks, world=1, rank=0, ko_sigma=0.1, ko_order=6)
+    a = ref.evolve(U, dt, 2)
+    b = dist_evo.evolve(U, dt, 2)
+    assert torch.equal(a, b)
+    assert dist_evo.constraint_norms(b) == ref.constraint_norms(a)
