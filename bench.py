@@ -67,7 +67,9 @@ def parse():
     ap.add_argument("--track", type=int, default=0,
                     help="after timing, evolve this many more steps and record the constraint norms")
     ap.add_argument("--track-every", type=int, default=10)
-    ap.add_argument("--ozaki-k", type=int, default=0, help="ozaki192: one digit count instead of k = 5..8")
+    ap.add_argument("--ozaki-k", type=int, default=0,
+                    help="ozaki192: one digit count instead of k = 5..8; amr3/amr4: evolve through the "
+                         "Ozaki INT8 derivative path with this many digit planes (0 = float64 stencils)")
     ap.add_argument("--ozaki-n", type=int, default=192, help="ozaki192: interior points per axis")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -456,6 +458,27 @@ def track_constraints(advance, norms, total: int, every: int):
     return out
 
 
+def _oz_kind(f, axis):
+    """Pass kind of field f along axis in the batched Ozaki bundle (ozaki.cu KINDS)."""
+    d2 = f in (0, 1) or 3 <= f < 12
+    return (0 if d2 else 1) if axis == 0 else ((2 if d2 else 3) if axis == 1 else 4)
+
+
+def _pool_drift(pool, A, B):
+    """Per field, over the interiors of all blocks: max |A - B| / max |B|."""
+    import torch
+    num = torch.zeros(24, dtype=torch.float64, device=A.device)
+    den = torch.zeros(24, dtype=torch.float64, device=A.device)
+    for i, b in enumerate(pool.blocks):
+        o = int(pool.offsets[i])
+        g = b.ng
+        a = A[o:o + 24 * b.points].view((24,) + tuple(b.shape))[:, g:-g, g:-g, g:-g]
+        r = B[o:o + 24 * b.points].view((24,) + tuple(b.shape))[:, g:-g, g:-g, g:-g]
+        num = torch.maximum(num, (a - r).abs().amax(dim=(1, 2, 3)))
+        den = torch.maximum(den, r.abs().amax(dim=(1, 2, 3)))
+    return [float(x) for x in (num / den.clamp_min(1e-300)).cpu()]
+
+
 def bench_amr(args):
     """A block-list workload: one persistent stage launch per RK4 stage over
     every block (plus the ghost fill per level with ghosts="exchange"), the
@@ -477,10 +500,15 @@ def bench_amr(args):
     blocks, punct, dt = amr.workload(index)
     pool = amr.BlockPool(blocks)
     U0 = torch.from_numpy(pool.initial_state(punct, seed=0)).to(dev)
+    oz_k = int(args.ozaki_k)
     t_plan = time.time()
-    evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=0, device=dev, ghosts=args.ghosts)
+    if oz_k:
+        from bssn3d_b200.ozaki import BatchedOzakiEvolution
+        evo = BatchedOzakiEvolution(pool, k=oz_k, ko_sigma=0.1, ko_order=6, device=dev, ghosts=args.ghosts)
+    else:
+        evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=0, device=dev, ghosts=args.ghosts)
     t_plan = time.time() - t_plan
-    tune = amr.autotune(evo, U0, dt)
+    tune = {} if oz_k else amr.autotune(evo, U0, dt)
     graph, U_g, S_g = evo.capture(U0, evo.scalars(0.0, dt))
 
     def barrier():
@@ -513,7 +541,16 @@ def bench_amr(args):
     interior = pool.interior_points
     value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
     fills = len(evo.dplan.fill) if evo.dplan is not None else 0
-    tracked = None
+    ghost_counts = evo.plan.counts if evo.plan is not None else None
+    variant = evo.variant
+    per_stage = 1 + fills
+    if oz_k:
+        evo.check()
+        # the bundle's passes with tiles, one stage launch
+        per_stage = fills + 1 + sum(1 for f in range(24) for a in range(3)
+                                    if evo.ntiles_kind[_oz_kind(f, a)] > 0) + 33
+    del graph
+    tracked = tracked_fp64 = drift = None
     if args.track > 0:
         # a fresh run from t = 0 on its own captured step
         g2, U2g, S2g = evo.capture(U0, evo.scalars(0.0, dt))
@@ -523,21 +560,42 @@ def bench_amr(args):
                 g2.replay()
         tracked = track_constraints(advance, lambda: evo.constraint_norms(U2g), args.track, args.track_every)
         del g2
+        if oz_k:
+            # the same run on the float64 stencils of the block path
+            evo.check()
+            U_oz = U2g.clone()
+            del evo, U2g, U_g
+            torch.cuda.empty_cache()
+            fp = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=0, device=dev, ghosts=args.ghosts)
+            g3, U3g, _ = fp.capture(U0, fp.scalars(0.0, dt))
+
+            def advance_fp(k):
+                for _ in range(k):
+                    g3.replay()
+            tracked_fp64 = track_constraints(advance_fp, lambda: fp.constraint_norms(U3g), args.track,
+                                             args.track_every)
+            del g3
+            drift = _pool_drift(pool, U_oz, U3g)
+    metric = METRIC.replace("RK4 step", "RK4 step over a block list")
+    if oz_k:
+        metric += f", Ozaki INT8 derivatives k={oz_k} + FP64 algebra"
     line = {
-        "metric": METRIC.replace("RK4 step", "RK4 step over a block list"), "value": value, "unit": UNIT,
+        "metric": metric, "value": value, "unit": UNIT,
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"{len(blocks)} Brill-Lindquist blocks, {len(set(b.level for b in blocks))} levels "
                                f"(amr.workload({index})), interiors 16^3/24^3/32^3 +3 ghosts",
                    "ghosts": args.ghosts, "interior_points": interior, "points": pool.points,
-                   "state_bytes": int(pool.size * 8), "variant": evo.variant,
+                   "state_bytes": int(pool.size * 8), "variant": None if oz_k else variant,
                    "autotune_ms": {str(k): v for k, v in tune.items()},
                    "plan_s": round(t_plan, 2), "parallelism": f"replicas x{world}"},
-        "clocks": clk, "gpu_launches": (4 * (1 + fills) + 1) * args.steps, "finite": finite,
-        "ghost_points": evo.plan.counts if evo.plan is not None else None,
+        "clocks": clk, "gpu_launches": (4 * per_stage + 1) * args.steps, "finite": finite,
+        "ghost_points": ghost_counts,
         "constraints": tracked, "roofline": None, "e2e": None, "cpu_baseline": None,
     }
-    del graph
+    if oz_k:
+        line["ozaki"] = {"k": oz_k, "constraints_fp64": tracked_fp64,
+                         "state_vs_fp64_after_track": drift}
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()

@@ -267,6 +267,39 @@ int bssn_b200_ozaki_derivatives(void* stream, const double* F, const double* S, 
                                 double ko_sigma, int ko_order, long long Sx, long long Sy,
                                 long long Sz, void* workspace, size_t workspace_bytes);
 
+/* Block-list form of the Ozaki path. Derivatives live in a slot pool D:
+ * nslot = 162 doubles per point with KO (ko_sigma > 0), else 138; slot s of
+ * block b starts at D + (offset_b / 24) * nslot + s * n_b, n_b = sx*sy*sz
+ * (the state pool's layout with nslot fields). Each block is differentiated
+ * on its own padded array with its own spacing; with core > 0 only the
+ * derivatives at [core, s - core)^3 are valid (the passes cover that box,
+ * plus the 3-point margins the mixed derivatives read).
+ *
+ * bssn_b200_batch_ozaki_plan: HOST tables in, HOST tables out. Fills
+ * host_tile0 (5 * nblocks ints: first tile of each block for each of the
+ * bundle's 5 pass kinds), host_ntiles (5 totals) and host_pts0 (nblocks
+ * prefix counts of covered points, for bssn_b200_batch_rk4_stage_derivs) and
+ * returns the covered point total, or -1 (bssn_b200_ozaki_last_error).
+ * Upload host_tile0 and host_pts0 to the device; pass host_ntiles as is.
+ * The workspace of the batched call is 256 bytes (the error flag at its start).
+ *
+ * bssn_b200_batch_rk4_stage_derivs: one RK4 stage (the update of
+ * bssn_b200_batch_rk4_stage) at the covered points from the derivatives in D
+ * (KO sums from D when ko_slots != 0), one thread per point. Errors:
+ * bssn_b200_last_error. No reference counterpart (the reference has neither
+ * BSSN AMR nor a BSSN Ozaki path). */
+long long bssn_b200_batch_ozaki_plan(const bssn_b200_block* host_blocks, int nblocks, int* host_tile0,
+                                     long long* host_ntiles, long long* host_pts0);
+int bssn_b200_batch_ozaki_derivatives(void* stream, const double* F, const double* S, double* D, int k,
+                                      double ko_sigma, int ko_order, const bssn_b200_block* blocks,
+                                      int nblocks, const int* tile0, const long long* host_ntiles,
+                                      void* workspace, size_t workspace_bytes);
+int bssn_b200_batch_rk4_stage_derivs(void* stream, int stage, const double* U, const double* Y,
+                                     double* ACC, double* YNEXT, const double* D, const double* S,
+                                     int ko_slots, double chi_floor, double alpha_floor,
+                                     const bssn_b200_block* blocks, int nblocks,
+                                     const long long* pts0, long long npoints);
+
 /* Algebraic enforcement in place (3D/src/bssn3d/evolve.py:93-119). */
 int bssn_b200_enforce(void* stream, double* U, long long npts, double chi_floor,
                       double alpha_floor);

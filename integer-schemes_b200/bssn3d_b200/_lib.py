@@ -46,6 +46,9 @@ _SIGNATURES = {
     "bssn_b200_ozaki_error_flag": ([_P, _LL, _LL, _LL, _I], _P),
     "bssn_b200_ozaki_last_error": ([], ctypes.c_char_p),
     "bssn_b200_ozaki_derivatives": ([_P, _P, _P, _P, _I, _D, _I, _LL, _LL, _LL, _P, _SZ], _I),
+    "bssn_b200_batch_ozaki_plan": ([_P, _I, _P, _P, _P], _LL),
+    "bssn_b200_batch_ozaki_derivatives": ([_P, _P, _P, _P, _I, _D, _I, _P, _I, _P, _P, _P, _SZ], _I),
+    "bssn_b200_batch_rk4_stage_derivs": ([_P, _I, _P, _P, _P, _P, _P, _P, _I, _D, _D, _P, _I, _P, _LL], _I),
     "bssn_b200_enforce": ([_P, _P, _LL, _D, _D], _I),
     "bssn_b200_periodic_sync": ([_P, _P, _LL, _LL, _LL, _I], _I),
 }

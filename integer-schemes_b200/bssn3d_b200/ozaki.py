@@ -13,6 +13,7 @@ from __future__ import annotations
 import torch
 
 from . import _lib
+from .amr import BatchedEvolution
 from .fused_rhs import _stream_handle
 
 
@@ -61,3 +62,93 @@ class OzakiDerivatives:
         _lib.check(_lib.load().bssn_b200_rhs_algebra(_stream_handle(self.device), Fs.data_ptr(),
                                                       D.data_ptr(), S_dev.data_ptr(), out.data_ptr(), npts))
         return out
+
+
+NKIND = 5  # pass kinds of one derivative bundle (bssn_b200_batch_ozaki_plan)
+
+
+def ozaki_plan(table, nblocks: int):
+    """Host plan of a block table for the batched Ozaki calls: (tile0 as a
+    flat list of 5 * nblocks first tiles, the 5 per-kind tile totals as a
+    ctypes array, pts0 as a list, covered point total)."""
+    import ctypes
+    lib = _lib.load()
+    tile0 = (ctypes.c_int * (NKIND * nblocks))()
+    ntiles = (ctypes.c_longlong * NKIND)()
+    pts0 = (ctypes.c_longlong * nblocks)()
+    npts = lib.bssn_b200_batch_ozaki_plan(ctypes.addressof(table), nblocks, tile0, ntiles, pts0)
+    if npts < 0:
+        raise _lib.BssnB200Error(_lib.EINVAL, lib.bssn_b200_ozaki_last_error().decode())
+    return list(tile0), ntiles, list(pts0), int(npts)
+
+
+class BatchedOzakiEvolution(BatchedEvolution):
+    """RK4 over a pooled block list with the Ozaki INT8 derivative path. Each
+    stage is the ghost fill (``ghosts="exchange"``), ONE derivative bundle of
+    every block (``bssn_b200_batch_ozaki_derivatives``: the 138 derivatives
+    and 24 KO sums into a pooled slot buffer, k digit planes per value) and
+    ONE stage update from those derivatives (``bssn_b200_batch_rk4_stage_derivs``:
+    the float64 algebra and the RK4 update at the covered points). The
+    FP64 path it is measured against is :class:`BatchedEvolution` on the same
+    pool; everything else (fills, restriction, norms, capture) is shared.
+    """
+
+    def __init__(self, pool, k: int, params=None, ko_sigma: float = 0.1, ko_order: int = 6,
+                 device="cuda", ghosts: str = "exchange", restrict: bool = False, plan=None, active=None):
+        super().__init__(pool, params=params, ko_sigma=ko_sigma, ko_order=ko_order, variant=0,
+                         device=device, ghosts=ghosts, restrict=restrict, plan=plan, active=active)
+        if not 1 <= int(k) <= 8:
+            raise ValueError(f"k must be 1..8, not {k}")
+        self.k = int(k)
+        table, _ = pool.descriptors(pool.tile, core=ghosts == "exchange", active=self.active)
+        n = len(self.active)
+        tile0, self.ntiles_kind, pts0, self.npoints = ozaki_plan(table, n)
+        raw = bytes(memoryview(table).cast("B"))
+        self.oz_table = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.device)
+        self.tile0_dev = torch.tensor(tile0, dtype=torch.int32, device=self.device)
+        self.pts0_dev = torch.tensor(pts0, dtype=torch.int64, device=self.device)
+        self.nslot = 162 if self.ko_sigma > 0 else 138
+        self.D = torch.empty(pool.size // 24 * self.nslot, dtype=torch.float64, device=self.device)
+        self.ws = torch.zeros(512, dtype=torch.uint8, device=self.device)
+        self.ws_ptr = self.ws.data_ptr() + (-self.ws.data_ptr()) % 256
+
+    def derivatives(self, Y, S):
+        """The derivative bundle of every block of Y into ``self.D``."""
+        lib = _lib.load()
+        rc = lib.bssn_b200_batch_ozaki_derivatives(self._stream(), Y.data_ptr(), S.data_ptr(), self.D.data_ptr(),
+                                                   self.k, self.ko_sigma, self.ko_order, self.oz_table.data_ptr(),
+                                                   len(self.active), self.tile0_dev.data_ptr(), self.ntiles_kind,
+                                                   self.ws_ptr, 256)
+        if rc != _lib.OK:
+            raise _lib.BssnB200Error(rc, lib.bssn_b200_ozaki_last_error().decode())
+        return self.D
+
+    def derivative_view(self, i: int):
+        """Block i's (nslot, sx, sy, sz) view of the derivative pool."""
+        b = self.pool.blocks[i]
+        o = int(self.pool.offsets[i]) // 24 * self.nslot
+        return self.D[o:o + self.nslot * b.points].view((self.nslot,) + tuple(b.shape))
+
+    def stage(self, stage, U, Y, ACC, YNEXT, S):
+        self.derivatives(Y, S)
+        p = self.params
+        rc = _lib.load().bssn_b200_batch_rk4_stage_derivs(
+            self._stream(), stage, U.data_ptr(), Y.data_ptr(), ACC.data_ptr(), YNEXT.data_ptr(), self.D.data_ptr(),
+            S.data_ptr(), int(self.ko_sigma > 0), p.chi_floor, p.alpha_floor, self.oz_table.data_ptr(),
+            len(self.active), self.pts0_dev.data_ptr(), self.npoints)
+        _lib.check(rc)
+
+    def check(self) -> None:
+        """Raise if a tensor-core wait gave up in any launch so far."""
+        off = self.ws_ptr - self.ws.data_ptr()
+        if self.ws[off:off + 4].view(torch.int32).item() != 0:
+            raise _lib.BssnB200Error(_lib.ECUDA, "Ozaki tensor-core wait gave up")
+
+    def rhs(self, U, S):
+        raise NotImplementedError("the Ozaki block-list path advances states; use BatchedEvolution.rhs")
+
+    def capture(self, U, S):
+        g, U_g, S_g = super().capture(U, S)
+        g.static_tensors = g.static_tensors + (self.D, self.ws, self.oz_table, self.tile0_dev, self.pts0_dev,
+                                               self.ntiles_kind)
+        return g, U_g, S_g

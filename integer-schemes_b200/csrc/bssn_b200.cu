@@ -320,7 +320,7 @@ __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c
 template <int R>
 __global__ void __launch_bounds__(NTHREADS) deriv_kernel(const Args args) {
   using Geo = TileGeom<R>;
-  extern __shared__ __align__(16) double smem[];
+  extern __shared__ __align__(128) double smem[];
   __shared__ Weights W;
   const int tid = threadIdx.x;
   init_weights<R>(W, args.S, args.ko_sigma, tid);
@@ -845,6 +845,80 @@ __global__ void __launch_bounds__(128) algebra_kernel(const double* __restrict__
     });
     auto emit = [&](int k, double v) { OUT[(long long)k * n + q] = v; };
     acc.finalize(fld, P, emit, NoCon());
+  }
+}
+
+// One RK4 stage from precomputed derivatives over the covered points
+// [core, s - core)^3 of every block of a block list: the algebra of
+// algebra_kernel on the stage input Y with the block's spacing and the stage
+// time, the KO sums taken from slots 138..161 of D when ko_slots is set, and
+// the stage epilogue of the stream kernel (evolve.py:125-131, the final stage
+// with algebraic enforcement). Derivative slot s of block b is at
+// D + (offset_b / 24) * nslot + s * n_b. Points are enumerated block by block
+// (pts0 = prefix of covered points), one thread per point.
+__global__ void __launch_bounds__(128) stage_derivs_kernel(
+    const double* __restrict__ U, const double* __restrict__ Y, double* __restrict__ ACC, double* __restrict__ OUT,
+    const double* __restrict__ D, int nslot, const double* __restrict__ S, int stage, int ko_slots,
+    double chi_floor, double alpha_floor, const bssn_b200_block* __restrict__ blocks, int nblocks,
+    const long long* __restrict__ pts0, long long npoints) {
+  const Params P0 = load_params(S);
+  const double cs = stage == 0 ? 0.0 : (stage == 3 ? 1.0 : 0.5);
+  const double dt = P0.dt;
+  const double hstep = (stage == 2) ? dt : 0.5 * dt;
+  const double w6 = dt / 6.0;
+  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npoints;
+       q += (long long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nblocks - 1;  // last block whose first point is <= q
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (pts0[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const bssn_b200_block bk = blocks[lo];
+    const int c = bk.core;
+    const int ey = bk.sy - 2 * c, ez = bk.sz - 2 * c;
+    const int lq = (int)(q - pts0[lo]);
+    const int z = lq % ez + c, y = (lq / ez) % ey + c, x = lq / (ez * ey) + c;
+    const long long n = (long long)bk.sx * bk.sy * bk.sz;
+    const long long p = ((long long)x * bk.sy + y) * bk.sz + z;
+    const long long gidx = bk.offset + p;
+    const double* Dq = D + (bk.offset / 24) * nslot + p;
+    Params P = P0;
+    P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
+    P.t = P0.t + cs * P0.dt;  // stage time t, t+dt/2, t+dt/2, t+dt (evolve.py:125-131)
+    auto fld = [&](int k) -> double { return __ldg(Y + gidx + (long long)k * n); };
+    auto drv = [&](int s) -> double { return __ldg(Dq + (long long)s * n); };
+    Stream<true, false> acc;
+    acc.init(fld);
+    Unroll<0, NFIELD>::run([&](auto ic) {
+      constexpr int f = stream_field(decltype(ic)::value);
+      double d1[3], d2[6];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) d1[a] = drv(d1slot(f, a));
+#pragma unroll
+      for (int pp = 0; pp < 6; ++pp) d2[pp] = has_d2(f) ? drv(d2slot(f, pp)) : 0.0;
+      acc.consume(f, d1, d2, ko_slots ? drv(138 + f) : 0.0, P, fld);
+    });
+    double* A = ACC + gidx;
+    double* O = OUT + gidx;
+    double en[14];
+#pragma unroll
+    for (int k = 0; k < 14; ++k) en[k] = 0.0;
+    auto emit = [&](int k, double rate) {
+      const long long o = (long long)k * n;
+      const double u = U[gidx + o];
+      if (stage == 0) {
+        A[o] = rate;
+        O[o] = u + hstep * rate;
+      } else if (stage < 3) {
+        A[o] = A[o] + 2.0 * rate;
+        O[o] = u + hstep * rate;
+      } else {
+        const double un = u + w6 * (A[o] + rate);
+        if (!hold_for_enforce(en, k, un)) O[o] = un;
+      }
+    };
+    acc.finalize(fld, P, emit, NoCon());
+    if (stage == 3) enforce_point(en, O, n, chi_floor, alpha_floor);
   }
 }
 
@@ -1377,6 +1451,32 @@ int bssn_b200_rhs_algebra(void* stream, const double* F, const double* D, const 
   bssn::algebra_kernel<<<(int)blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(F, D, S, OUT, npts);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_fail("rhs_algebra launch", e);
+  return 0;
+}
+
+int bssn_b200_batch_rk4_stage_derivs(void* stream, int stage, const double* U, const double* Y, double* ACC,
+                                     double* YNEXT, const double* D, const double* S, int ko_slots,
+                                     double chi_floor, double alpha_floor, const bssn_b200_block* blocks,
+                                     int nblocks, const long long* pts0, long long npoints) {
+  if (stage < 0 || stage > 3) return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: stage must be 0..3");
+  if (!U || !Y || !ACC || !YNEXT || !D || !S || !blocks || !pts0)
+    return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: NULL operand");
+  if (YNEXT == Y) return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: YNEXT must not alias Y");
+  if (stage < 3 && YNEXT == U) return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: YNEXT may alias U only at stage 3");
+  if (ACC == Y || ACC == U || ACC == YNEXT)
+    return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: ACC must not alias another operand");
+  if (nblocks < 1 || npoints < 1) return fail(BSSN_B200_EINVAL, "batch_rk4_stage_derivs: empty block list");
+  int sms = 0;
+  int rc = device_sms(&sms);
+  if (rc) return rc;
+  long long grid = (npoints + 127) / 128;
+  const long long cap = (long long)sms * 16;
+  if (grid > cap) grid = cap;
+  bssn::stage_derivs_kernel<<<(int)grid, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+      U, Y, ACC, YNEXT, D, ko_slots ? 162 : 138, S, stage, ko_slots ? 1 : 0, chi_floor, alpha_floor, blocks, nblocks,
+      pts0, npoints);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail("batch_rk4_stage_derivs launch", e);
   return 0;
 }
 

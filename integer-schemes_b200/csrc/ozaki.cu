@@ -63,25 +63,26 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 // Instruction descriptor: S32 accumulator, signed INT8 A and B, both K-major, N=64, M=128.
 constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NCOL >> 3) << 17) | ((128u >> 4) << 24);
 
-struct Line {
-  int len;           // points along the axis
-  long long nlines;  // product of the other two extents
-  long long stride;  // element stride along the axis
+// The passes of one derivative bundle over a block with ghost margin `core`
+// (core = 0 on a single grid): the differentiation axis and how far the
+// covered box reaches past the core on each axis. First derivatives along x
+// and y of the fields with second derivatives are taken 3 points into the
+// ghosts across the line, where the mixed passes read them back.
+struct PassKind {
+  int axis;
+  int ext[3];
 };
+constexpr int NKIND = 5;
+constexpr PassKind KINDS[NKIND] = {{0, {0, 3, 3}}, {0, {0, 0, 0}}, {1, {0, 0, 3}}, {1, {0, 0, 0}}, {2, {0, 0, 0}}};
 
-__host__ __device__ inline Line line_geom(int axis, long long Sx, long long Sy, long long Sz) {
-  Line L;
-  if (axis == 0) { L.len = (int)Sx; L.nlines = Sy * Sz; L.stride = Sy * Sz; }
-  else if (axis == 1) { L.len = (int)Sy; L.nlines = Sx * Sz; L.stride = Sz; }
-  else { L.len = (int)Sz; L.nlines = Sx * Sy; L.stride = 1; }
-  return L;
-}
-
-// Offset of the first element of line l (lines ordered with z fastest).
-__device__ __forceinline__ long long line_base(int axis, long long l, long long Sy, long long Sz) {
-  if (axis == 0) return l;                                   // l = y*Sz + z
-  if (axis == 1) return (l / Sz) * Sy * Sz + (l % Sz);       // l = x*Sz + z
-  return l * Sz;                                             // l = x*Sy + y
+// Tiles of one pass over one block: 128-line groups x 16-output groups.
+inline long long pass_tiles(const bssn_b200_block& b, const PassKind& k) {
+  const int s[3] = {b.sx, b.sy, b.sz};
+  long long e[3];
+  for (int q = 0; q < 3; ++q) e[q] = s[q] - 2LL * (b.core - k.ext[q] > 0 ? b.core - k.ext[q] : 0);
+  const int ax = k.axis;
+  const long long nlines = e[(ax + 1) % 3] * e[(ax + 2) % 3];
+  return ((nlines + LT - 1) / LT) * ((e[ax] + NO - 1) / NO);
 }
 
 // ---- fused split + contraction + recombination -----------------------------
@@ -100,17 +101,26 @@ constexpr int FT = 256;       // threads of the fused kernel
 constexpr int FW = 33;        // float64 window pitch (conflict-free rows)
 constexpr int OP = 17;        // output staging pitch
 
+// Sources and destinations are slots of per-block pools: slot s of block b
+// starts at pool + (offset_b / 24) * slots + s * n_b, n_b = sx*sy*sz (the
+// block layout of bssn_b200_block, whose offsets count 24-field states). A
+// single grid is one block at offset 0, passed by value in `one`.
 struct FusedArgs {
   const double* src;
-  int axis;
-  long long Sx, Sy, Sz;
-  int R, k, ko_reach;
-  const double* S;
+  int src_slots, src_slot;
+  double* dst;
+  int dst_slots;
+  int d1_slot, d2_slot, ko_slot;  // -1: not written
+  int ko_add;                     // add the KO term to the slot instead of storing it
+  int k;
+  const double* S;                // scalar pack (device); a single grid's spacing is S[13 + axis]
   double ko_sigma;
-  double* d1;
-  double* d2;
-  double* ko;
-  int ko_add;
+  int ext[3];                     // the pass covers [core - ext, s - core + ext) per axis (clamped to the array)
+  bssn_b200_block one;            // the single grid (blocks == nullptr)
+  const bssn_b200_block* blocks;  // block list (device) or nullptr
+  int nblocks;
+  const int* tile0;               // block list: first tile of each block along this axis (device)
+  long long ntiles;
   int* err;
 };
 
@@ -137,12 +147,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     if (tid == 0) atomicExch(a.err, 1);
     return;
   }
-  const Line L = line_geom(AXIS, a.Sx, a.Sy, a.Sz);
   constexpr int KWL = NO + 2 * R;  // window positions the stencils use (22 or 24)
-  const double h = a.S[13 + AXIS];
-  const double w1 = (1.0 / 60.0) * (1.0 / h);
-  const double w2 = (1.0 / 180.0) * (1.0 / (h * h));
-  const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / h);
   {
     const int c1[7] = {-1, 9, -45, 0, 45, -9, 1};
     const int c2h[7] = {0, 0, 2, -4, 2, 0, 0};       // 270 = 2*128 + 14, -490 = -4*128 + 22
@@ -178,39 +183,95 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = tmem_base;
 
-  const long long nlb = (L.nlines + LT - 1) / LT;
-  const int nzt = (L.len + NO - 1) / NO;
-  const long long ntiles = nlb * nzt;
   constexpr bool zaxis = AXIS == 2;
-  // the window of tile t into F[buf] (edge-clamped positions, tail lines repeat
-  // the last line); the lines' first elements are tabled once per tile. Ends
-  // in a barrier-free state: callers place it right after a barrier.
+  // Geometry of tile t: its block; the box of the block the pass covers
+  // ([m, s - m) per axis, m = max(core - ext, 0)); the box's lines along AXIS
+  // (the other two axes, "slow" and "fast" in memory order); the tile's
+  // 128-line group lb and first output z0; the pool bases of its slots.
+  struct TileInfo {
+    long long lb, nlines, stride, st_slow, st_fast;
+    long long pbase, n;  // block start in points, points per block
+    int z0, len, s_axis, m_axis, e_fast, m_slow, m_fast;
+    double h;
+  };
+  auto tile_info = [&](long long t) -> TileInfo {
+    TileInfo ti;
+    long long lt = t, offset = 0;
+    int s[3] = {a.one.sx, a.one.sy, a.one.sz}, core = 0;
+    if (a.blocks) {
+      int lo = 0, hi = a.nblocks - 1;  // last block whose first tile is <= t
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (a.tile0[mid] <= t) lo = mid; else hi = mid - 1;
+      }
+      const bssn_b200_block* bk = a.blocks + lo;
+      s[0] = bk->sx; s[1] = bk->sy; s[2] = bk->sz;
+      core = bk->core;
+      offset = bk->offset;
+      ti.h = bk->h[AXIS];
+      lt = t - a.tile0[lo];
+    } else {
+      ti.h = a.S[13 + AXIS];
+    }
+    int m[3], e[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      m[q] = core - a.ext[q] > 0 ? core - a.ext[q] : 0;
+      e[q] = s[q] - 2 * m[q];
+    }
+    constexpr int SLOW = AXIS == 0 ? 1 : 0, FAST = AXIS == 2 ? 1 : 2;
+    const long long st[3] = {(long long)s[1] * s[2], (long long)s[2], 1};
+    ti.len = e[AXIS];
+    ti.s_axis = s[AXIS];
+    ti.m_axis = m[AXIS];
+    ti.stride = st[AXIS];
+    ti.nlines = (long long)e[SLOW] * e[FAST];
+    ti.e_fast = e[FAST];
+    ti.m_slow = m[SLOW];
+    ti.m_fast = m[FAST];
+    ti.st_slow = st[SLOW];
+    ti.st_fast = st[FAST];
+    const int nzt = (ti.len + NO - 1) / NO;
+    ti.lb = lt / nzt;
+    ti.z0 = (int)(lt % nzt) * NO;
+    ti.n = (long long)s[0] * s[1] * s[2];
+    ti.pbase = offset / 24;
+    return ti;
+  };
+  // the window of tile t into F[buf] (positions clamped to the block's array,
+  // its edge padding; tail lines repeat the last line); the lines' first
+  // elements (block-local, axis coordinate 0) are tabled once per tile.
+  // Callers place it right after a barrier.
   auto load_window = [&](long long t, int buf) {
-    const long long lb = t / nzt;
-    const int z0 = (int)(t % nzt) * NO;
+    const TileInfo ti = tile_info(t);
     if (tid < LT) {
-      long long l = lb * LT + tid;
-      if (l >= L.nlines) l = L.nlines - 1;
-      sm.base[buf][tid] = line_base(AXIS, l, a.Sy, a.Sz);
+      long long l = ti.lb * LT + tid;
+      if (l >= ti.nlines) l = ti.nlines - 1;
+      const int slow = (int)(l / ti.e_fast), fast = (int)(l % ti.e_fast);
+      sm.base[buf][tid] = (long long)(slow + ti.m_slow) * ti.st_slow + (long long)(fast + ti.m_fast) * ti.st_fast;
     }
     __syncthreads();
+    const double* src = a.src + ti.pbase * a.src_slots + (long long)a.src_slot * ti.n;
     for (int i = tid; i < LT * KWL; i += FT) {
       const int r = zaxis ? i / KWL : i % LT;
       const int pos = zaxis ? i % KWL : i / LT;
-      int q = z0 - R + pos;
-      q = q < 0 ? 0 : (q > L.len - 1 ? L.len - 1 : q);  // edge padding (derivatives.py:83-84)
-      cp_async8(&sm.F[buf][r * FW + pos], a.src + sm.base[buf][r] + (long long)q * L.stride);
+      int q = ti.m_axis + ti.z0 - R + pos;
+      q = q < 0 ? 0 : (q > ti.s_axis - 1 ? ti.s_axis - 1 : q);  // edge padding (derivatives.py:83-84)
+      cp_async8(&sm.F[buf][r * FW + pos], src + sm.base[buf][r] + (long long)q * ti.stride);
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
+  const long long ntiles = a.ntiles;
   uint32_t phase = 0;
   bool failed = false;
   long long tile = blockIdx.x;
   if (tile < ntiles) load_window(tile, 0);
   int buf = 0;
   for (; tile < ntiles && !failed; tile += gridDim.x, buf ^= 1) {
-    const long long lb = tile / nzt;
-    const int z0 = (int)(tile % nzt) * NO;
+    const TileInfo ti = tile_info(tile);
+    const double w1 = (1.0 / 60.0) * (1.0 / ti.h);
+    const double w2 = (1.0 / 180.0) * (1.0 / (ti.h * ti.h));
+    const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / ti.h);
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     // ---- exponent and digits: threads r and r + 128 take the two 16-position halves of line r ----
@@ -323,13 +384,16 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     for (int i = tid; i < LT * NO; i += FT) {
       const int rr = zaxis ? i / NO : i % LT;
       const int o = zaxis ? i % NO : i / LT;
-      const long long l = lb * LT + rr;
-      const int z = z0 + o;
-      if (l < L.nlines && z < L.len && !failed) {
-        const long long pt = sm.base[buf][rr] + (long long)z * L.stride;
-        if (a.d1) a.d1[pt] = sm.O[0][rr * OP + o];
-        if (a.d2) a.d2[pt] = sm.O[1][rr * OP + o];
-        if (a.ko) a.ko[pt] = a.ko_add ? a.ko[pt] + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
+      const long long l = ti.lb * LT + rr;
+      const int z = ti.z0 + o;
+      if (l < ti.nlines && z < ti.len && !failed) {
+        double* out = a.dst + ti.pbase * a.dst_slots + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride;
+        if (a.d1_slot >= 0) out[(long long)a.d1_slot * ti.n] = sm.O[0][rr * OP + o];
+        if (a.d2_slot >= 0) out[(long long)a.d2_slot * ti.n] = sm.O[1][rr * OP + o];
+        if (a.ko_slot >= 0) {
+          double* kp = out + (long long)a.ko_slot * ti.n;
+          *kp = a.ko_add ? *kp + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
+        }
       }
     }
     __syncthreads();  // TMEM columns, digits and output staging are reused by the next tile
@@ -362,6 +426,75 @@ int oz_fail(int code, const std::string& m) {
   g_oz_err = m;
   return code;
 }
+
+bool has_d2(int f) { return f == 0 || f == 1 || (f >= 3 && f < 12); }
+int g2slot(int f) { return f == 0 ? 0 : (f == 1 ? 1 : (f < 9 ? 2 + f - 3 : 8 + f - 9)); }
+
+// One derivative bundle (138 slots, +24 KO sums) of the 24 fields of F into
+// the slot pool D: per field and axis one pass giving the first derivative,
+// the diagonal second derivative and the KO term (added over the axes), then
+// the mixed second derivatives as first derivatives of the x and y first
+// derivatives (derivative_bundle.py:31-48). `one` is the single grid when
+// blocks == nullptr; else tile0 holds NKIND tables of nblocks first tiles.
+int run_bundle(cudaStream_t st, const double* F, const double* S, double* D, int k, double ko_sigma,
+               int ko_order, const bssn_b200_block& one, const bssn_b200_block* blocks, int nblocks,
+               const int* tile0, const long long* ntiles, int* err) {
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return oz_fail(BSSN_B200_EINVAL, "ozaki: device ordinal out of range");
+  e = cudaMemsetAsync(err, 0, sizeof(int), st);
+  if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
+  const bool use_ko = ko_sigma > 0.0;
+  const int R = (use_ko && ko_order == 8) ? 4 : 3;
+  const int nslot = use_ko ? 162 : 138;
+  auto pass = [&](const double* src, int src_slots, int src_slot, int kind, int d1, int d2, int ko,
+                  int ko_add) -> int {
+    const ozaki::PassKind& pk = ozaki::KINDS[kind];
+    ozaki::FusedArgs m{};
+    m.src = src; m.src_slots = src_slots; m.src_slot = src_slot;
+    m.dst = D; m.dst_slots = nslot; m.d1_slot = d1; m.d2_slot = d2; m.ko_slot = ko; m.ko_add = ko_add;
+    m.k = k; m.S = S; m.ko_sigma = use_ko ? ko_sigma : 0.0;
+    for (int q = 0; q < 3; ++q) m.ext[q] = pk.ext[q];
+    m.one = one; m.blocks = blocks; m.nblocks = nblocks;
+    m.tile0 = blocks ? tile0 + (long long)kind * nblocks : nullptr;
+    m.ntiles = ntiles[kind];
+    m.err = err;
+    if (m.ntiles < 1) return 0;
+    const int grid = (int)(m.ntiles < sms ? m.ntiles : sms);  // one CTA per SM: it owns all 512 TMEM columns
+    cudaError_t le;
+    const int axis = pk.axis;
+    if (R == 4)
+      le = axis == 0 ? launch_fused<4, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<4, 1>(m, grid, st, dev)
+                                                                        : launch_fused<4, 2>(m, grid, st, dev));
+    else
+      le = axis == 0 ? launch_fused<3, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<3, 1>(m, grid, st, dev)
+                                                                        : launch_fused<3, 2>(m, grid, st, dev));
+    if (le == cudaSuccess) le = cudaGetLastError();
+    if (le != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki launch: ") + cudaGetErrorString(le));
+    return 0;
+  };
+  const int diag[3] = {0, 3, 5};
+  for (int f = 0; f < 24; ++f) {
+    for (int axis = 0; axis < 3; ++axis) {
+      const bool d2f = has_d2(f);
+      const int kind = axis == 0 ? (d2f ? 0 : 1) : (axis == 1 ? (d2f ? 2 : 3) : 4);
+      const int d2 = d2f ? 72 + 6 * g2slot(f) + diag[axis] : -1;
+      int rc = pass(F, 24, f, kind, 3 * f + axis, d2, use_ko ? 138 + f : -1, axis > 0);
+      if (rc) return rc;
+    }
+  }
+  for (int f = 0; f < 24; ++f) {
+    if (!has_d2(f)) continue;
+    const int g = 72 + 6 * g2slot(f);
+    int rc = pass(D, nslot, 3 * f + 0, 3, g + 1, -1, -1, 0);   // d/dy of d/dx
+    if (!rc) rc = pass(D, nslot, 3 * f + 0, 4, g + 2, -1, -1, 0);  // d/dz of d/dx
+    if (!rc) rc = pass(D, nslot, 3 * f + 1, 4, g + 4, -1, -1, 0);  // d/dz of d/dy
+    if (rc) return rc;
+  }
+  return 0;
+}
 }  // namespace
 
 extern "C" {
@@ -379,73 +512,87 @@ int* bssn_b200_ozaki_error_flag(void* workspace, long long Sx, long long Sy, lon
   return reinterpret_cast<int*>(static_cast<char*>(workspace) + need - 256);
 }
 
+static int check_common(int k, double ko_sigma, int ko_order, void* workspace, size_t workspace_bytes) {
+  if (k < 1 || k > ozaki::MAXK) return oz_fail(BSSN_B200_EINVAL, "ozaki: k must be 1..8");
+  if (ko_sigma > 0.0 && ko_order != 6 && ko_order != 8) return oz_fail(BSSN_B200_EINVAL, "ozaki: ko_order must be 6 or 8");
+  if (workspace_bytes < 256) return oz_fail(BSSN_B200_EINVAL, "ozaki: workspace smaller than bssn_b200_ozaki_workspace_bytes()");
+  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return oz_fail(BSSN_B200_EINVAL, "ozaki: workspace not 256-byte aligned");
+  return 0;
+}
+
 int bssn_b200_ozaki_derivatives(void* stream, const double* F, const double* S, double* DOUT, int k,
                                 double ko_sigma, int ko_order, long long Sx, long long Sy, long long Sz,
                                 void* workspace, size_t workspace_bytes) {
   if (!F || !S || !DOUT || !workspace) return oz_fail(BSSN_B200_EINVAL, "ozaki: NULL operand");
-  if (k < 1 || k > ozaki::MAXK) return oz_fail(BSSN_B200_EINVAL, "ozaki: k must be 1..8");
   if (Sx < 8 || Sy < 8 || Sz < 8) return oz_fail(BSSN_B200_EINVAL, "ozaki: every extent must be >= 8");
   if (Sx * Sy * Sz > (1LL << 31)) return oz_fail(BSSN_B200_EINVAL, "ozaki: grid too large");
-  const bool use_ko = ko_sigma > 0.0;
-  if (use_ko && ko_order != 6 && ko_order != 8) return oz_fail(BSSN_B200_EINVAL, "ozaki: ko_order must be 6 or 8");
-  const size_t need = bssn_b200_ozaki_workspace_bytes(Sx, Sy, Sz, k);
-  if (workspace_bytes < need) return oz_fail(BSSN_B200_EINVAL, "ozaki: workspace smaller than bssn_b200_ozaki_workspace_bytes()");
-  if ((reinterpret_cast<uintptr_t>(workspace) & 255) != 0) return oz_fail(BSSN_B200_EINVAL, "ozaki: workspace not 256-byte aligned");
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  int dev = 0, sms = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
-  // One CTA per SM: the fused kernel owns all 512 TMEM columns.
-  if (dev < 0 || dev >= 64) return oz_fail(BSSN_B200_EINVAL, "ozaki: device ordinal out of range");
+  int rc = check_common(k, ko_sigma, ko_order, workspace, workspace_bytes);
+  if (rc) return rc;
+  if (workspace_bytes < bssn_b200_ozaki_workspace_bytes(Sx, Sy, Sz, k))
+    return oz_fail(BSSN_B200_EINVAL, "ozaki: workspace smaller than bssn_b200_ozaki_workspace_bytes()");
+  bssn_b200_block one{};
+  one.sx = (int)Sx; one.sy = (int)Sy; one.sz = (int)Sz;
+  one.h[0] = one.h[1] = one.h[2] = 1.0;  // the spacing comes from S[13..15]
+  long long nt[ozaki::NKIND];
+  for (int q = 0; q < ozaki::NKIND; ++q) nt[q] = ozaki::pass_tiles(one, ozaki::KINDS[q]);
   int* err = bssn_b200_ozaki_error_flag(workspace, Sx, Sy, Sz, k);
-  e = cudaMemsetAsync(err, 0, sizeof(int), st);
-  if (e != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki: ") + cudaGetErrorString(e));
-  const long long n = Sx * Sy * Sz;
-  const int R = (use_ko && ko_order == 8) ? 4 : 3;
-  auto pass = [&](const double* src, int axis, double* d1, double* d2, double* ko, int ko_add) -> int {
-    const ozaki::Line L = ozaki::line_geom(axis, Sx, Sy, Sz);
-    ozaki::FusedArgs m{};
-    m.src = src; m.axis = axis; m.Sx = Sx; m.Sy = Sy; m.Sz = Sz;
-    m.R = R; m.k = k; m.ko_reach = R; m.S = S; m.ko_sigma = use_ko ? ko_sigma : 0.0;
-    m.d1 = d1; m.d2 = d2; m.ko = ko; m.ko_add = ko_add; m.err = err;
-    const long long tiles = ((L.nlines + ozaki::LT - 1) / ozaki::LT) * ((L.len + ozaki::NO - 1) / ozaki::NO);
-    const int grid = (int)(tiles < sms ? tiles : sms);
-    cudaError_t le;
-    if (R == 4)
-      le = axis == 0 ? launch_fused<4, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<4, 1>(m, grid, st, dev)
-                                                                        : launch_fused<4, 2>(m, grid, st, dev));
-    else
-      le = axis == 0 ? launch_fused<3, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<3, 1>(m, grid, st, dev)
-                                                                        : launch_fused<3, 2>(m, grid, st, dev));
-    if (le == cudaSuccess) le = cudaGetLastError();
-    if (le != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki launch: ") + cudaGetErrorString(le));
-    return 0;
-  };
-  auto has_d2 = [](int f) { return f == 0 || f == 1 || (f >= 3 && f < 12); };
-  auto g2slot = [](int f) { return f == 0 ? 0 : (f == 1 ? 1 : (f < 9 ? 2 + f - 3 : 8 + f - 9)); };
-  const int diag[3] = {0, 3, 5};
-  for (int f = 0; f < 24; ++f) {
-    for (int axis = 0; axis < 3; ++axis) {
-      double* d1 = DOUT + (long long)(3 * f + axis) * n;
-      double* d2 = has_d2(f) ? DOUT + (long long)(72 + 6 * g2slot(f) + diag[axis]) * n : nullptr;
-      double* ko = use_ko ? DOUT + (long long)(138 + f) * n : nullptr;
-      int rc = pass(F + (long long)f * n, axis, d1, d2, ko, axis > 0);
-      if (rc) return rc;
+  return run_bundle(static_cast<cudaStream_t>(stream), F, S, DOUT, k, ko_sigma, ko_order, one, nullptr, 0,
+                    nullptr, nt, err);
+}
+
+long long bssn_b200_batch_ozaki_plan(const bssn_b200_block* host_blocks, int nblocks, int* host_tile0,
+                                     long long* host_ntiles, long long* host_pts0) {
+  if (!host_blocks || nblocks < 1 || !host_tile0 || !host_ntiles || !host_pts0) {
+    oz_fail(BSSN_B200_EINVAL, "batch_ozaki_plan: NULL or empty table");
+    return -1;
+  }
+  long long t[ozaki::NKIND] = {0, 0, 0, 0, 0}, pts = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    const bssn_b200_block& bk = host_blocks[b];
+    if (bk.sx < 8 || bk.sy < 8 || bk.sz < 8 || bk.offset < 0 || bk.offset % 24 != 0 || !(bk.h[0] > 0) ||
+        !(bk.h[1] > 0) || !(bk.h[2] > 0)) {
+      oz_fail(BSSN_B200_EINVAL, "batch_ozaki_plan: block " + std::to_string(b) +
+                                    " has an extent below 8, a bad offset or a bad spacing");
+      return -1;
+    }
+    if ((long long)bk.sx * bk.sy * bk.sz >= (1LL << 31)) {
+      oz_fail(BSSN_B200_EINVAL, "batch_ozaki_plan: block " + std::to_string(b) + " has 2^31 points or more");
+      return -1;
+    }
+    if (bk.core < 0 || 2 * bk.core >= bk.sx || 2 * bk.core >= bk.sy || 2 * bk.core >= bk.sz) {
+      oz_fail(BSSN_B200_EINVAL, "batch_ozaki_plan: block " + std::to_string(b) + " has a core margin that leaves no points");
+      return -1;
+    }
+    host_pts0[b] = pts;
+    pts += (long long)(bk.sx - 2 * bk.core) * (bk.sy - 2 * bk.core) * (bk.sz - 2 * bk.core);
+    for (int q = 0; q < ozaki::NKIND; ++q) {
+      host_tile0[(long long)q * nblocks + b] = (int)t[q];
+      t[q] += ozaki::pass_tiles(bk, ozaki::KINDS[q]);
+      if (t[q] >= (1LL << 31)) {
+        oz_fail(BSSN_B200_EINVAL, "batch_ozaki_plan: too many tiles");
+        return -1;
+      }
     }
   }
-  // mixed second derivatives: the first derivative along the lower axis,
-  // differentiated again along the higher one (derivative_bundle.py:31-48)
-  for (int f = 0; f < 24; ++f) {
-    if (!has_d2(f)) continue;
-    const double* tx = DOUT + (long long)(3 * f + 0) * n;
-    const double* ty = DOUT + (long long)(3 * f + 1) * n;
-    int rc = pass(tx, 1, DOUT + (long long)(72 + 6 * g2slot(f) + 1) * n, nullptr, nullptr, 0);
-    if (!rc) rc = pass(tx, 2, DOUT + (long long)(72 + 6 * g2slot(f) + 2) * n, nullptr, nullptr, 0);
-    if (!rc) rc = pass(ty, 2, DOUT + (long long)(72 + 6 * g2slot(f) + 4) * n, nullptr, nullptr, 0);
-    if (rc) return rc;
-  }
-  return 0;
+  for (int q = 0; q < ozaki::NKIND; ++q) host_ntiles[q] = t[q];
+  return pts;
+}
+
+int bssn_b200_batch_ozaki_derivatives(void* stream, const double* F, const double* S, double* D, int k,
+                                      double ko_sigma, int ko_order, const bssn_b200_block* blocks,
+                                      int nblocks, const int* tile0, const long long* host_ntiles,
+                                      void* workspace, size_t workspace_bytes) {
+  if (!F || !S || !D || !blocks || !tile0 || !host_ntiles || !workspace || nblocks < 1)
+    return oz_fail(BSSN_B200_EINVAL, "batch_ozaki_derivatives: NULL operand or empty table");
+  int rc = check_common(k, ko_sigma, ko_order, workspace, workspace_bytes);
+  if (rc) return rc;
+  for (int q = 0; q < ozaki::NKIND; ++q)
+    if (host_ntiles[q] < 0 || host_ntiles[q] >= (1LL << 31))
+      return oz_fail(BSSN_B200_EINVAL, "batch_ozaki_derivatives: tile count out of range");
+  bssn_b200_block one{};
+  int* err = static_cast<int*>(workspace);
+  return run_bundle(static_cast<cudaStream_t>(stream), F, S, D, k, ko_sigma, ko_order, one, blocks, nblocks,
+                    tile0, host_ntiles, err);
 }
 
 }  // extern "C"
