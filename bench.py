@@ -67,6 +67,7 @@ def parse():
     ap.add_argument("--track", type=int, default=0,
                     help="after timing, evolve this many more steps and record the constraint norms")
     ap.add_argument("--track-every", type=int, default=10)
+    ap.add_argument("--blocks", type=int, default=0, help="amr3/amr4: block count instead of 600/2000 (small cases)")
     ap.add_argument("--ozaki-k", type=int, default=0,
                     help="ozaki192: one digit count instead of k = 5..8; amr3/amr4: evolve through the "
                          "Ozaki INT8 derivative path with this many digit planes (0 = float64 stencils)")
@@ -497,7 +498,7 @@ def bench_amr(args):
     from bssn3d_b200 import amr
 
     index = int(args.workload[-1])
-    blocks, punct, dt = amr.workload(index)
+    blocks, punct, dt = amr.workload(index, count=args.blocks or None)
     pool = amr.BlockPool(blocks)
     U0 = torch.from_numpy(pool.initial_state(punct, seed=0)).to(dev)
     oz_k = int(args.ozaki_k)

@@ -5,11 +5,13 @@
 // 3D/src/multipatch/amr/sync.py:70-122 cross-level and same-level fills),
 // applied to the BSSN block pool that the batched stage kernels evolve.
 //
-// A fill is a host-planned list of boxes (bssn_b200_fill_op). One launch
-// executes one list: every thread takes one destination point (flattened
-// over the boxes by a prefix of box volumes, found by binary search) and
-// moves all 24 fields. The work is a gather of a small part of the pool per
-// stage, so the kernel is bound by memory latency and sized to fill the SMs.
+// A fill is a host-planned list of boxes (bssn_b200_fill_op), copies and
+// injections first, prolongations after. A call executes one list as two
+// launches, one per range: every thread takes one destination point
+// (flattened over the boxes by a prefix of box volumes, its box found by
+// binary search) and moves all 24 fields. The work is a gather of a small
+// part of the pool, latency-bound: the copy kernel needs few registers and
+// runs five CTAs per SM, the prolongation kernel two.
 //
 // Prolongation refines the source block x, then y, then z. A point odd on an
 // axis sums its 6 taps in offset order starting from 0 (the reference's
@@ -20,6 +22,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <string>
 
@@ -37,71 +40,108 @@ struct Wmid {
 
 __device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
 
-__global__ void __launch_bounds__(NTHREADS) fill_kernel(double* __restrict__ pool,
-                                                        const bssn_b200_fill_op* __restrict__ ops,
-                                                        int nops, long long npoints, const Wmid W) {
+// A level's boxes are ordered copy and restriction first, prolongation after
+// (bssn_b200_fill_plan orders them): two kernels take the two ranges, so the
+// copies run with the few registers they need and many warps in flight.
+__device__ __forceinline__ int first_prolong(const bssn_b200_fill_op* __restrict__ ops, int nops) {
+  int lo = 0, hi = nops;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (ops[mid].kind == BSSN_B200_FILL_PROLONG) hi = mid; else lo = mid + 1;
+  }
+  return lo;
+}
+
+// Destination point (d0, d1, d2) of point p in box op, or false past the box.
+__device__ __forceinline__ bool decode(const bssn_b200_fill_op& op, long long p, int& d0, int& d1, int& d2) {
+  const int bz = op.hi[2] - op.lo[2], by = op.hi[1] - op.lo[1];
+  int r = (int)(p - op.point0);  // box volumes stay below 2^31 (checked by the plan)
+  d2 = op.lo[2] + r % bz;
+  r /= bz;
+  d1 = op.lo[1] + r % by;
+  d0 = op.lo[0] + r / by;
+  return d0 < op.hi[0];  // npoints past the plan's total: nothing to write
+}
+
+__device__ __forceinline__ void copy_point(double* __restrict__ pool, const bssn_b200_fill_op& op, long long p) {
+  int d0, d1, d2;
+  if (!decode(op, p, d0, d1, d2)) return;
+  const int ss1 = op.src_s[1], ss2 = op.src_s[2];
+  const long long nd = (long long)op.dst_s[0] * op.dst_s[1] * op.dst_s[2];
+  const long long ns = (long long)op.src_s[0] * ss1 * ss2;
+  double* dst = pool + op.dst_off + ((long long)d0 * op.dst_s[1] + d1) * op.dst_s[2] + d2;
+  const int m = op.kind == BSSN_B200_FILL_RESTRICT ? 2 : 1;
+  const double* src = pool + op.src_off + ((long long)(m * d0 + op.shift[0]) * ss1 + (m * d1 + op.shift[1])) * ss2 +
+                      (m * d2 + op.shift[2]);
+#pragma unroll 8
+  for (int f = 0; f < NFIELD; ++f) dst[f * nd] = src[f * ns];
+}
+
+__device__ __forceinline__ void prolong_point(double* __restrict__ pool, const bssn_b200_fill_op& op, long long p,
+                                              const double* __restrict__ w) {
+  int d0, d1, d2;
+  if (!decode(op, p, d0, d1, d2)) return;
+  const int ss0 = op.src_s[0], ss1 = op.src_s[1], ss2 = op.src_s[2];
+  const long long nd = (long long)op.dst_s[0] * op.dst_s[1] * op.dst_s[2];
+  const long long ns = (long long)ss0 * ss1 * ss2;
+  double* dst = pool + op.dst_off + ((long long)d0 * op.dst_s[1] + d1) * op.dst_s[2] + d2;
+  const double* src = pool + op.src_off;
+  // per axis: 1 tap (even, coincident node) or 6 taps (odd, midpoint)
+  const int g0 = d0 + op.shift[0], g1 = d1 + op.shift[1], g2 = d2 + op.shift[2];
+  const bool o0 = g0 & 1, o1 = g1 & 1, o2 = g2 & 1;
+  const int k0 = g0 >> 1, k1 = g1 >> 1, k2 = g2 >> 1;  // arithmetic shift: floor(g / 2)
+  const int ny = o1 ? 6 : 1, nz = o2 ? 6 : 1;
+  const long long sxs = (long long)ss1 * ss2;
+  for (int f = 0; f < NFIELD; ++f) {
+    const double* P = src + f * ns;
+    double vz = 0.0;
+    for (int c = 0; c < nz; ++c) {
+      const int iz = clampi(o2 ? k2 - 2 + c : k2, ss2 - 1);
+      double vy = 0.0;
+      for (int b = 0; b < ny; ++b) {
+        const int iy = clampi(o1 ? k1 - 2 + b : k1, ss1 - 1);
+        const double* row = P + (long long)iy * ss2 + iz;
+        double vx;
+        if (!o0) {
+          vx = row[k0 < 0 ? 0 : (k0 > ss0 - 1 ? ss0 - 1 : k0) * sxs];
+        } else {
+          vx = 0.0;
+#pragma unroll
+          for (int a = 0; a < 6; ++a) vx = __dadd_rn(vx, __dmul_rn(w[a], row[clampi(k0 - 2 + a, ss0 - 1) * sxs]));
+        }
+        vy = o1 ? __dadd_rn(vy, __dmul_rn(w[b], vx)) : vx;
+      }
+      vz = o2 ? __dadd_rn(vz, __dmul_rn(w[c], vy)) : vy;
+    }
+    dst[f * nd] = vz;
+  }
+}
+
+// One kernel per kind range: every thread takes points p of the range by a
+// grid stride and finds its box by binary search over the range's boxes.
+template <bool PROLONG>
+__global__ void __launch_bounds__(NTHREADS, PROLONG ? 2 : 5) fill_kernel(double* __restrict__ pool,
+                                                                         const bssn_b200_fill_op* __restrict__ ops,
+                                                                         int nops, long long npoints, const Wmid W) {
+  __shared__ double sw[6];  // midpoint weights (indexed by tap)
+  if (PROLONG && threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < 6; ++j) sw[j] = W.w[j];
+  }
+  if (PROLONG) __syncthreads();
+  const int jp = first_prolong(ops, nops);
+  const int j_lo = PROLONG ? jp : 0, j_hi = PROLONG ? nops : jp;
+  if (j_lo >= j_hi) return;
+  const long long p_hi = j_hi < nops ? ops[j_hi].point0 : npoints;
   const long long stride = (long long)gridDim.x * NTHREADS;
-  for (long long p = (long long)blockIdx.x * NTHREADS + threadIdx.x; p < npoints; p += stride) {
-    int lo = 0, hi = nops - 1;  // last op with point0 <= p
+  for (long long p = ops[j_lo].point0 + (long long)blockIdx.x * NTHREADS + threadIdx.x; p < p_hi; p += stride) {
+    int lo = j_lo, hi = j_hi - 1;  // last box of the range with point0 <= p
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (ops[mid].point0 <= p) lo = mid; else hi = mid - 1;
     }
-    const bssn_b200_fill_op& op = ops[lo];
-    const int bz = op.hi[2] - op.lo[2], by = op.hi[1] - op.lo[1];
-    long long r = p - op.point0;
-    const int d2 = op.lo[2] + (int)(r % bz);
-    r /= bz;
-    const int d1 = op.lo[1] + (int)(r % by);
-    const int d0 = op.lo[0] + (int)(r / by);
-    if (d0 >= op.hi[0]) continue;  // npoints past the plan's total: nothing to write
-    const int ss0 = op.src_s[0], ss1 = op.src_s[1], ss2 = op.src_s[2];
-    const long long nd = (long long)op.dst_s[0] * op.dst_s[1] * op.dst_s[2];
-    const long long ns = (long long)ss0 * ss1 * ss2;
-    double* dst = pool + op.dst_off + ((long long)d0 * op.dst_s[1] + d1) * op.dst_s[2] + d2;
-    const double* src = pool + op.src_off;
-    if (op.kind != BSSN_B200_FILL_PROLONG) {
-      const int m = op.kind == BSSN_B200_FILL_RESTRICT ? 2 : 1;
-      const long long s = ((long long)(m * d0 + op.shift[0]) * ss1 + (m * d1 + op.shift[1])) * ss2 +
-                          (m * d2 + op.shift[2]);
-#pragma unroll 4
-      for (int f = 0; f < NFIELD; ++f) dst[f * nd] = src[s + f * ns];
-      continue;
-    }
-    // per axis: 1 tap (even, coincident node) or 6 taps (odd, midpoint)
-    const int g0 = d0 + op.shift[0], g1 = d1 + op.shift[1], g2 = d2 + op.shift[2];
-    const bool o0 = g0 & 1, o1 = g1 & 1, o2 = g2 & 1;
-    const int k0 = g0 >> 1, k1 = g1 >> 1, k2 = g2 >> 1;  // arithmetic shift: floor(g / 2)
-    int ix[6], iy[6], iz[6];
-#pragma unroll
-    for (int j = 0; j < 6; ++j) {
-      ix[j] = clampi(o0 ? k0 - 2 + j : k0, ss0 - 1);
-      iy[j] = clampi(o1 ? k1 - 2 + j : k1, ss1 - 1);
-      iz[j] = clampi(o2 ? k2 - 2 + j : k2, ss2 - 1);
-    }
-    const int ny = o1 ? 6 : 1, nz = o2 ? 6 : 1;
-    const long long sxs = (long long)ss1 * ss2;
-    for (int f = 0; f < NFIELD; ++f) {
-      const double* P = src + f * ns;
-      double vz = 0.0;
-      for (int c = 0; c < nz; ++c) {
-        double vy = 0.0;
-        for (int b = 0; b < ny; ++b) {
-          const double* row = P + (long long)iy[b] * ss2 + iz[c];
-          double vx;
-          if (!o0) {
-            vx = row[ix[0] * sxs];
-          } else {
-            vx = 0.0;
-#pragma unroll
-            for (int a = 0; a < 6; ++a) vx = __dadd_rn(vx, __dmul_rn(W.w[a], row[ix[a] * sxs]));
-          }
-          vy = o1 ? __dadd_rn(vy, __dmul_rn(W.w[b], vx)) : vx;
-        }
-        vz = o2 ? __dadd_rn(vz, __dmul_rn(W.w[c], vy)) : vy;
-      }
-      dst[f * nd] = vz;
-    }
+    if (PROLONG) prolong_point(pool, ops[lo], p, sw);
+    else copy_point(pool, ops[lo], p);
   }
 }
 
@@ -148,6 +188,10 @@ long long bssn_b200_fill_plan(bssn_b200_fill_op* host_ops, int nops, long long p
       ns *= op.src_s[a];
       vol *= op.hi[a] - op.lo[a];
     }
+    if (vol >= (1LL << 31)) {
+      fail(BSSN_B200_EINVAL, at + "box of 2^31 points or more");
+      return -1;
+    }
     if (op.dst_off < 0 || op.src_off < 0 || op.dst_off + 24 * nd > pool_doubles || op.src_off + 24 * ns > pool_doubles) {
       fail(BSSN_B200_EINVAL, at + "block outside the pool");
       return -1;
@@ -156,8 +200,15 @@ long long bssn_b200_fill_plan(bssn_b200_fill_op* host_ops, int nops, long long p
       fail(BSSN_B200_EINVAL, at + "a block cannot fill itself");
       return -1;
     }
+  }
+  // copies and injections first, prolongations after (the fill launches one
+  // kernel per range); boxes of one list never overlap, so order is free
+  std::stable_partition(host_ops, host_ops + nops,
+                        [](const bssn_b200_fill_op& o) { return o.kind != BSSN_B200_FILL_PROLONG; });
+  for (int i = 0; i < nops; ++i) {
+    bssn_b200_fill_op& op = host_ops[i];
     op.point0 = total;
-    total += vol;
+    total += (long long)(op.hi[0] - op.lo[0]) * (op.hi[1] - op.lo[1]) * (op.hi[2] - op.lo[2]);
   }
   return total;
 }
@@ -173,9 +224,13 @@ int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int
   int rc = bssn_host::device_sms(&sms);
   if (rc) return rc;
   const long long want = (npoints + amr::NTHREADS - 1) / amr::NTHREADS;
-  const int grid = (int)(want < 8LL * sms ? want : 8LL * sms);
-  amr::fill_kernel<<<grid, amr::NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(pool, ops, nops, npoints, W);
+  const long long cap_c = 5LL * 2 * sms, cap_p = 2LL * 2 * sms;  // two waves of resident CTAs
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  amr::fill_kernel<false><<<(int)(want < cap_c ? want : cap_c), amr::NTHREADS, 0, st>>>(pool, ops, nops, npoints, W);
   cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return bssn_host::cuda_fail("fill launch", e);
+  amr::fill_kernel<true><<<(int)(want < cap_p ? want : cap_p), amr::NTHREADS, 0, st>>>(pool, ops, nops, npoints, W);
+  e = cudaGetLastError();
   if (e != cudaSuccess) return bssn_host::cuda_fail("fill launch", e);
   return 0;
 }

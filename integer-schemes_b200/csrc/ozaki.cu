@@ -2,14 +2,16 @@
 //
 // Every finite-difference stencil of the BSSN bundle is a banded matrix with
 // small integer coefficients (C1 x60, C2 x180, KO6 x64, KO8 x256). A float64
-// field is split, line by line along the differentiation axis, into k signed
-// INT8 digits under one shared power-of-two exponent per line,
-//     f = 2^e * sum_s q_s 2^(-7(s+1)),   |q_s| <= 64,   |f| 2^-e < 1/2,
+// field is split, line by line along the differentiation axis, into k INT8
+// digits under one shared power-of-two exponent per line: with |f| 2^-e < 1/2,
+//     X = rint(f 2^(7k-e)) = q_0 2^(7(k-1)) + sum_{s>0} q_s 2^(7(k-1-s)),
+// q_0 = X >> 7(k-1) signed (|q_0| <= 64), q_s the 7-bit groups of X's two's
+// complement below it (0 <= q_s < 128), so f ~ 2^e sum_s q_s 2^(-7(s+1));
 // the stencil is applied to every digit plane as an exact INT8 x INT8 -> INT32
 // tensor-core contraction, and the digit results are recombined in float64.
 // The contraction is exact and the recombination order is fixed, so results
-// are bit-reproducible run to run; the only approximation is the split
-// (|residual| <= 2^(e-7k-1) per value, e the window's exponent).
+// are bit-reproducible run to run; the only approximation is the rounding of
+// X (|residual| <= 2^(e-7k-1) per value, e the window's exponent).
 //
 // This follows the banded-integer-stencil design of the reference's MCS
 // Ozaki derivative (2D/src/mcs2d/schemes/ozaki.py:286-323: stencil matrix,
@@ -41,7 +43,7 @@ constexpr int MAXK = 8;
 constexpr int LT = 128;           // lines per tile (MMA M)
 constexpr int NO = 16;            // outputs per tile along the axis
 constexpr int KW = 32;            // K window in padded positions
-constexpr int NCOL = 4 * NO;      // MMA N: C1 | C2 hi | C2 lo | KO
+constexpr int NCOL = 4 * NO;      // widest MMA N: C1 | C2 hi | C2 lo | KO
 constexpr long long WAIT_LIMIT = 1LL << 26;  // bounded mbarrier polls (~1 s)
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -61,7 +63,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
 }
 
 // Instruction descriptor: S32 accumulator, signed INT8 A and B, both K-major, N=64, M=128.
-constexpr uint32_t IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NCOL >> 3) << 17) | ((128u >> 4) << 24);
+__host__ __device__ constexpr uint32_t idesc(int n) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((128u >> 4) << 24);
+}
 
 // The passes of one derivative bundle over a block with ghost margin `core`
 // (core = 0 on a single grid): the differentiation axis and how far the
@@ -136,8 +140,14 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
 
-template <int R, int AXIS>
+// D2: the pass also gives the diagonal second derivative (C2 as a high and a
+// low INT8 digit); KOG: it also gives the KO term. The MMA's N holds only the
+// stencil groups the pass needs: C1 [| C2 hi | C2 lo] [| KO], 16 columns each.
+template <int R, int AXIS, bool D2, bool KOG>
 __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
+  constexpr int NG = 1 + (D2 ? 2 : 0) + (KOG ? 1 : 0);
+  constexpr int NC = NO * NG;       // MMA N and TMEM columns per digit plane
+  constexpr int GKO = D2 ? 3 : 1;   // column group of KO
   extern __shared__ __align__(128) unsigned char fsm_raw[];
   FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fsm_raw);
   __shared__ __align__(8) uint64_t mbar;
@@ -154,9 +164,10 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     const int c2l[7] = {2, -27, 14, 22, 14, -27, 2};
     const int k6[7] = {1, -6, 15, -20, 15, -6, 1};
     const int k8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1};
-    for (int i = tid; i < NCOL * KW; i += FT) {
+    for (int i = tid; i < NC * KW; i += FT) {
       const int n = i / KW, kb = i % KW;
-      const int st = n / NO, o = n % NO;
+      const int g = n / NO, o = n % NO;
+      const int st = (KOG && g == GKO) ? 3 : g;  // 0 C1, 1 C2 hi, 2 C2 lo, 3 KO
       const int j = kb - R - o;
       int v = 0;
       if (st < 3) {
@@ -166,7 +177,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       } else {
         if (j >= -3 && j <= 3) v = k6[j + 3];
       }
-      sm.B[canon(n, kb, NCOL)] = (int8_t)v;
+      sm.B[canon(n, kb, NC)] = (int8_t)v;
     }
   }
   if (tid == 0) {
@@ -232,8 +243,9 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     ti.st_slow = st[SLOW];
     ti.st_fast = st[FAST];
     const int nzt = (ti.len + NO - 1) / NO;
-    ti.lb = lt / nzt;
-    ti.z0 = (int)(lt % nzt) * NO;
+    const int lti = (int)lt;  // tile counts stay below 2^31 (checked on the host)
+    ti.lb = lti / nzt;
+    ti.z0 = (lti % nzt) * NO;
     ti.n = (long long)s[0] * s[1] * s[2];
     ti.pbase = offset / 24;
     return ti;
@@ -242,12 +254,11 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   // its edge padding; tail lines repeat the last line); the lines' first
   // elements (block-local, axis coordinate 0) are tabled once per tile.
   // Callers place it right after a barrier.
-  auto load_window = [&](long long t, int buf) {
-    const TileInfo ti = tile_info(t);
+  auto load_window = [&](const TileInfo& ti, int buf) {
     if (tid < LT) {
-      long long l = ti.lb * LT + tid;
-      if (l >= ti.nlines) l = ti.nlines - 1;
-      const int slow = (int)(l / ti.e_fast), fast = (int)(l % ti.e_fast);
+      int l = (int)ti.lb * LT + tid;  // lines of a block stay below 2^31
+      if (l >= ti.nlines) l = (int)ti.nlines - 1;
+      const int slow = l / ti.e_fast, fast = l % ti.e_fast;
       sm.base[buf][tid] = (long long)(slow + ti.m_slow) * ti.st_slow + (long long)(fast + ti.m_fast) * ti.st_fast;
     }
     __syncthreads();
@@ -265,10 +276,14 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   uint32_t phase = 0;
   bool failed = false;
   long long tile = blockIdx.x;
-  if (tile < ntiles) load_window(tile, 0);
+  TileInfo next{};
+  if (tile < ntiles) {
+    next = tile_info(tile);
+    load_window(next, 0);
+  }
   int buf = 0;
   for (; tile < ntiles && !failed; tile += gridDim.x, buf ^= 1) {
-    const TileInfo ti = tile_info(tile);
+    const TileInfo ti = next;
     const double w1 = (1.0 / 60.0) * (1.0 / ti.h);
     const double w2 = (1.0 / 180.0) * (1.0 / (ti.h * ti.h));
     const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / ti.h);
@@ -297,16 +312,18 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
 #pragma unroll
       for (int s2 = 0; s2 < MAXK; ++s2) wd[s2][0] = wd[s2][1] = wd[s2][2] = wd[s2][3] = 0u;
 #pragma unroll
+      const double p7k = ldexp(1.0, 7 * a.k);
       for (int j = 0; j < 16; ++j) {
         const int pos = 16 * half + j;
-        double rr = pos < KWL ? Fr[pos] * isc : 0.0;
+        // X = rint(f 2^(7k - e)), |X| <= 2^(7k-1); two's complement gives
+        // X = top 2^(7(k-1)) + sum_j d_j 2^(7j), 0 <= d_j < 128, |top| <= 64
+        const long long X = pos < KWL ? __double2ll_rn((Fr[pos] * isc) * p7k) : 0;
 #pragma unroll
         for (int s2 = 0; s2 < MAXK; ++s2) {
           if (s2 < a.k) {
-            const double t = rr * 128.0;
-            const double d = rint(t);
-            rr = t - d;
-            wd[s2][j >> 2] |= (uint32_t)(uint8_t)(int8_t)(int)d << (8 * (j & 3));
+            const long long sh = X >> (7 * (a.k - 1 - s2));
+            const int d = s2 == 0 ? (int)sh : (int)(sh & 127);
+            wd[s2][j >> 2] |= (uint32_t)(d & 255) << (8 * (j & 3));
           }
         }
       }
@@ -318,15 +335,18 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     // ---- prefetch the next tile's window; thread 0 issues the contractions ----
-    if (tile + gridDim.x < ntiles) load_window(tile + gridDim.x, buf ^ 1);
+    if (tile + gridDim.x < ntiles) {
+      next = tile_info(tile + gridDim.x);
+      load_window(next, buf ^ 1);
+    }
     if (tid == 0) {
-      const uint64_t db = smem_desc(smem_u32(sm.B), NCOL * 16, 128);
+      const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
       for (int s2 = 0; s2 < a.k; ++s2) {
         const uint64_t da = smem_desc(smem_u32(&sm.A[s2][0]), LT * 16, 128);
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NCOL * s2)),
-            "l"(da), "l"(db), "r"(IDESC), "r"(0u));
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NC * s2)),
+            "l"(da), "l"(db), "r"(idesc(NC)), "r"(0u));
       }
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
                        smem_u32(&mbar))
@@ -354,21 +374,21 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     for (int o = 0; o < 8; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
     double w = ldexp(1.0, -7 * a.k);  // weight of the smallest digit plane
     for (int s2 = a.k - 1; s2 >= 0; --s2, w *= 128.0) {
-      uint32_t v[4][8];
+      uint32_t v[NG][8];
 #pragma unroll
-      for (int st = 0; st < 4; ++st) {
-        const uint32_t addr = tmem + lane + (uint32_t)(NCOL * s2 + NO * st + oc);
+      for (int g = 0; g < NG; ++g) {
+        const uint32_t addr = tmem + lane + (uint32_t)(NC * s2 + NO * g + oc);
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                     : "=r"(v[st][0]), "=r"(v[st][1]), "=r"(v[st][2]), "=r"(v[st][3]), "=r"(v[st][4]),
-                       "=r"(v[st][5]), "=r"(v[st][6]), "=r"(v[st][7])
+                     : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3]), "=r"(v[g][4]),
+                       "=r"(v[g][5]), "=r"(v[g][6]), "=r"(v[g][7])
                      : "r"(addr));
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
       for (int o = 0; o < 8; ++o) {
         r1[o] += (double)(int)v[0][o] * w;
-        r2[o] += (double)((int)v[1][o] * 128 + (int)v[2][o]) * w;
-        rk[o] += (double)(int)v[3][o] * w;
+        if (D2) r2[o] += (double)((int)v[D2 ? 1 : 0][o] * 128 + (int)v[D2 ? 2 : 0][o]) * w;
+        if (KOG) rk[o] += (double)(int)v[KOG ? GKO : 0][o] * w;
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -376,8 +396,8 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
 #pragma unroll
     for (int o = 0; o < 8; ++o) {
       sm.O[0][r * OP + oc + o] = (r1[o] * sc) * w1;
-      sm.O[1][r * OP + oc + o] = (r2[o] * sc) * w2;
-      sm.O[2][r * OP + oc + o] = (rk[o] * sc) * wko;
+      if (D2) sm.O[1][r * OP + oc + o] = (r2[o] * sc) * w2;
+      if (KOG) sm.O[2][r * OP + oc + o] = (rk[o] * sc) * wko;
     }
     __syncthreads();
     // ---- coalesced stores of the tile's outputs ----
@@ -388,9 +408,9 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       const int z = ti.z0 + o;
       if (l < ti.nlines && z < ti.len && !failed) {
         double* out = a.dst + ti.pbase * a.dst_slots + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride;
-        if (a.d1_slot >= 0) out[(long long)a.d1_slot * ti.n] = sm.O[0][rr * OP + o];
-        if (a.d2_slot >= 0) out[(long long)a.d2_slot * ti.n] = sm.O[1][rr * OP + o];
-        if (a.ko_slot >= 0) {
+        out[(long long)a.d1_slot * ti.n] = sm.O[0][rr * OP + o];
+        if (D2) out[(long long)a.d2_slot * ti.n] = sm.O[1][rr * OP + o];
+        if (KOG) {
           double* kp = out + (long long)a.ko_slot * ti.n;
           *kp = a.ko_add ? *kp + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
         }
@@ -410,17 +430,28 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
 namespace {
 thread_local std::string g_oz_err;
 
-template <int R, int AXIS>
+template <int R, int AXIS, bool D2, bool KOG>
 cudaError_t launch_fused(const ozaki::FusedArgs& m, int grid, cudaStream_t st, int dev) {
   static bool attr_done[64] = {false};
   constexpr int kSmem = (int)sizeof(ozaki::FusedSmem);
   if (!attr_done[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    cudaError_t e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS, D2, KOG>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
     if (e != cudaSuccess) return e;
     attr_done[dev] = true;
   }
-  ozaki::fused_kernel<R, AXIS><<<grid, ozaki::FT, kSmem, st>>>(m);
+  ozaki::fused_kernel<R, AXIS, D2, KOG><<<grid, ozaki::FT, kSmem, st>>>(m);
   return cudaSuccess;
+}
+
+// The instantiation for a pass: the KO reach only matters when KO is formed.
+template <int AXIS>
+cudaError_t launch_axis(const ozaki::FusedArgs& m, int grid, cudaStream_t st, int dev, int R, bool d2, bool ko) {
+  if (ko) {
+    if (R == 4) return d2 ? launch_fused<4, AXIS, true, true>(m, grid, st, dev) : launch_fused<4, AXIS, false, true>(m, grid, st, dev);
+    return d2 ? launch_fused<3, AXIS, true, true>(m, grid, st, dev) : launch_fused<3, AXIS, false, true>(m, grid, st, dev);
+  }
+  return d2 ? launch_fused<3, AXIS, true, false>(m, grid, st, dev) : launch_fused<3, AXIS, false, false>(m, grid, st, dev);
 }
 int oz_fail(int code, const std::string& m) {
   g_oz_err = m;
@@ -463,14 +494,11 @@ int run_bundle(cudaStream_t st, const double* F, const double* S, double* D, int
     m.err = err;
     if (m.ntiles < 1) return 0;
     const int grid = (int)(m.ntiles < sms ? m.ntiles : sms);  // one CTA per SM: it owns all 512 TMEM columns
-    cudaError_t le;
     const int axis = pk.axis;
-    if (R == 4)
-      le = axis == 0 ? launch_fused<4, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<4, 1>(m, grid, st, dev)
-                                                                        : launch_fused<4, 2>(m, grid, st, dev));
-    else
-      le = axis == 0 ? launch_fused<3, 0>(m, grid, st, dev) : (axis == 1 ? launch_fused<3, 1>(m, grid, st, dev)
-                                                                        : launch_fused<3, 2>(m, grid, st, dev));
+    const bool has2 = d2 >= 0, hasko = ko >= 0;
+    cudaError_t le = axis == 0 ? launch_axis<0>(m, grid, st, dev, R, has2, hasko)
+                   : (axis == 1 ? launch_axis<1>(m, grid, st, dev, R, has2, hasko)
+                                : launch_axis<2>(m, grid, st, dev, R, has2, hasko));
     if (le == cudaSuccess) le = cudaGetLastError();
     if (le != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki launch: ") + cudaGetErrorString(le));
     return 0;

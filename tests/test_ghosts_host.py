@@ -143,9 +143,14 @@ def test_device_table_layout_and_c_validation():
     for _, ops in plan.fill_lists:
         arr = (G.FillOp * len(ops))(*ops)
         total = lib.bssn_b200_fill_plan(ctypes.addressof(arr), len(ops), pool.size)
-        vols = [(o.hi[0] - o.lo[0]) * (o.hi[1] - o.lo[1]) * (o.hi[2] - o.lo[2]) for o in ops]
+        vols = [(o.hi[0] - o.lo[0]) * (o.hi[1] - o.lo[1]) * (o.hi[2] - o.lo[2]) for o in arr]
         assert total == sum(vols)
         assert [a.point0 for a in arr] == list(np.cumsum([0] + vols[:-1]))
+        kinds = [a.kind for a in arr]   # copies and injections first, prolongations after, stable
+        assert kinds == sorted(kinds, key=lambda k: k == G.PROLONG)
+        key = lambda o: (o.dst_off, o.src_off, tuple(o.lo), tuple(o.hi), o.kind)
+        assert sorted(map(key, arr)) == sorted(map(key, ops))
+        assert [key(a) for a in arr if a.kind != G.PROLONG] == [key(o) for o in ops if o.kind != G.PROLONG]
     ops = plan.fill_lists[-1][1]
     bad = [(lambda o: setattr(o, "kind", 7), "kind"),
            (lambda o: o.hi.__setitem__(0, o.dst_s[0] + 1), "box"),

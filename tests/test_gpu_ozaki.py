@@ -94,3 +94,20 @@ def test_ozaki_rejects_bad_arguments():
                                          10, 10, 10, ws.data_ptr(), 1 << 20)
     assert rc == _lib.EINVAL
     assert "k must be" in lib.bssn_b200_ozaki_last_error().decode()
+
+
+@pytest.mark.parametrize("k,ko_order", [(5, 6), (6, 8), (8, 6)])
+def test_ozaki_bundle_equals_cpu_restatement_bit_for_bit(k, ko_order):
+    """Every slot of the tensor-core bundle equals the numpy restatement of the
+    same digit split, integer contraction and recombination order."""
+    from bssn3d_b200.fused_rhs import device_scalars
+    from bssn3d_b200.ozaki import OzakiDerivatives
+    from oracle import ozaki_oracle as Z
+    grid, U, dt = _state(n=12)
+    Sd = device_scalars(_S(grid, dt), torch.device("cuda"))
+    oz = OzakiDerivatives(U.shape[1:], k)
+    got = oz.derivatives(torch.from_numpy(U).cuda(), Sd, ko_sigma=0.1, ko_order=ko_order).cpu().numpy()
+    oz.check()
+    want = Z.bundle(U, (grid.dx, grid.dy, grid.dz), k, ko_sigma=0.1, ko_order=ko_order)
+    bad = [s for s in range(162) if not np.array_equal(got[s], want[s])]
+    assert not bad, bad[:10]

@@ -51,6 +51,26 @@ def test_whole_blocks_equal_single_grid_bundle(ko_order):
         assert torch.equal(evo.derivative_view(i), ref), i
 
 
+def test_covered_interiors_equal_cpu_restatement():
+    """With ghost exchange every block's interior slots equal the numpy
+    restatement of the passes over that block's covered boxes, bit for bit."""
+    from bssn3d_b200.ozaki import BatchedOzakiEvolution
+    from oracle import ozaki_oracle as Z
+    pool, punct = _pool(count=6)
+    Y = torch.from_numpy(pool.initial_state(punct, seed=1)).cuda()
+    evo = BatchedOzakiEvolution(pool, k=6, ko_sigma=0.1, ko_order=6, ghosts="exchange")
+    evo.fill(Y)
+    evo.derivatives(Y, evo.scalars(0.0, 0.01))
+    torch.cuda.synchronize()
+    evo.check()
+    for i, blk in enumerate(pool.blocks):
+        g = blk.ng
+        want = Z.bundle(_block(pool, Y, i).cpu().numpy(), blk.h, 6, ko_sigma=0.1, ko_order=6, core=g)
+        got = evo.derivative_view(i).cpu().numpy()
+        I = (slice(None),) + (slice(g, -g),) * 3
+        assert np.array_equal(got[I], want[I]), i
+
+
 def test_covered_interiors_match_fp64_derivatives():
     from bssn3d_b200.fused_rhs import derivatives
     from bssn3d_b200.ozaki import BatchedOzakiEvolution
