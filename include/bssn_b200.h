@@ -155,7 +155,7 @@ int bssn_b200_batch_rk4_stage(void* stream, int stage, const double* U, const do
  * after (stable; boxes of one list are disjoint, so the order is free), fills
  * each op's point0 with the prefix of box volumes and returns the total point
  * count, or -1 (with bssn_b200_last_error). Upload the filled table for
- * bssn_b200_fill, which relies on that order. */
+ * bssn_b200_fill. */
 long long bssn_b200_fill_plan(bssn_b200_fill_op* host_ops, int nops, long long pool_doubles);
 
 /* Executes one planned list of fill boxes on `pool` (one launch, one thread

@@ -6,12 +6,12 @@
 // applied to the BSSN block pool that the batched stage kernels evolve.
 //
 // A fill is a host-planned list of boxes (bssn_b200_fill_op), copies and
-// injections first, prolongations after. A call executes one list as two
-// launches, one per range: every thread takes one destination point
+// injections first, prolongations after (fewer warps mix the two paths). One
+// launch executes one list: every thread takes one destination point
 // (flattened over the boxes by a prefix of box volumes, its box found by
 // binary search) and moves all 24 fields. The work is a gather of a small
-// part of the pool, latency-bound: the copy kernel needs few registers and
-// runs five CTAs per SM, the prolongation kernel two.
+// part of the pool and bound by memory latency: the copy path issues its 24
+// loads before its stores, and the grid holds four CTAs per SM.
 //
 // Prolongation refines the source block x, then y, then z. A point odd on an
 // axis sums its 6 taps in offset order starting from 0 (the reference's
@@ -33,24 +33,13 @@ namespace amr {
 
 constexpr int NFIELD = 24;
 constexpr int NTHREADS = 256;
+constexpr int MIN_CTAS = 4;  // resident CTAs per SM the register budget allows
 
 struct Wmid {
   double w[6];
 };
 
 __device__ __forceinline__ int clampi(int v, int hi) { return v < 0 ? 0 : (v > hi ? hi : v); }
-
-// A level's boxes are ordered copy and restriction first, prolongation after
-// (bssn_b200_fill_plan orders them): two kernels take the two ranges, so the
-// copies run with the few registers they need and many warps in flight.
-__device__ __forceinline__ int first_prolong(const bssn_b200_fill_op* __restrict__ ops, int nops) {
-  int lo = 0, hi = nops;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (ops[mid].kind == BSSN_B200_FILL_PROLONG) hi = mid; else lo = mid + 1;
-  }
-  return lo;
-}
 
 // Destination point (d0, d1, d2) of point p in box op, or false past the box.
 __device__ __forceinline__ bool decode(const bssn_b200_fill_op& op, long long p, int& d0, int& d1, int& d2) {
@@ -73,8 +62,11 @@ __device__ __forceinline__ void copy_point(double* __restrict__ pool, const bssn
   const int m = op.kind == BSSN_B200_FILL_RESTRICT ? 2 : 1;
   const double* src = pool + op.src_off + ((long long)(m * d0 + op.shift[0]) * ss1 + (m * d1 + op.shift[1])) * ss2 +
                       (m * d2 + op.shift[2]);
-#pragma unroll 8
-  for (int f = 0; f < NFIELD; ++f) dst[f * nd] = src[f * ns];
+  double v[NFIELD];  // all 24 loads in flight before the stores
+#pragma unroll
+  for (int f = 0; f < NFIELD; ++f) v[f] = src[f * ns];
+#pragma unroll
+  for (int f = 0; f < NFIELD; ++f) dst[f * nd] = v[f];
 }
 
 __device__ __forceinline__ void prolong_point(double* __restrict__ pool, const bssn_b200_fill_op& op, long long p,
@@ -117,30 +109,25 @@ __device__ __forceinline__ void prolong_point(double* __restrict__ pool, const b
   }
 }
 
-// One kernel per kind range: every thread takes points p of the range by a
-// grid stride and finds its box by binary search over the range's boxes.
-template <bool PROLONG>
-__global__ void __launch_bounds__(NTHREADS, PROLONG ? 2 : 5) fill_kernel(double* __restrict__ pool,
-                                                                         const bssn_b200_fill_op* __restrict__ ops,
-                                                                         int nops, long long npoints, const Wmid W) {
+// Every thread takes points p by a grid stride and finds its box by binary
+// search over the boxes' point prefix.
+__global__ void __launch_bounds__(NTHREADS, MIN_CTAS) fill_kernel(double* __restrict__ pool,
+                                                                  const bssn_b200_fill_op* __restrict__ ops,
+                                                                  int nops, long long npoints, const Wmid W) {
   __shared__ double sw[6];  // midpoint weights (indexed by tap)
-  if (PROLONG && threadIdx.x == 0) {
+  if (threadIdx.x == 0) {
 #pragma unroll
     for (int j = 0; j < 6; ++j) sw[j] = W.w[j];
   }
-  if (PROLONG) __syncthreads();
-  const int jp = first_prolong(ops, nops);
-  const int j_lo = PROLONG ? jp : 0, j_hi = PROLONG ? nops : jp;
-  if (j_lo >= j_hi) return;
-  const long long p_hi = j_hi < nops ? ops[j_hi].point0 : npoints;
+  __syncthreads();
   const long long stride = (long long)gridDim.x * NTHREADS;
-  for (long long p = ops[j_lo].point0 + (long long)blockIdx.x * NTHREADS + threadIdx.x; p < p_hi; p += stride) {
-    int lo = j_lo, hi = j_hi - 1;  // last box of the range with point0 <= p
+  for (long long p = (long long)blockIdx.x * NTHREADS + threadIdx.x; p < npoints; p += stride) {
+    int lo = 0, hi = nops - 1;  // last box with point0 <= p
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (ops[mid].point0 <= p) lo = mid; else hi = mid - 1;
     }
-    if (PROLONG) prolong_point(pool, ops[lo], p, sw);
+    if (ops[lo].kind == BSSN_B200_FILL_PROLONG) prolong_point(pool, ops[lo], p, sw);
     else copy_point(pool, ops[lo], p);
   }
 }
@@ -224,13 +211,10 @@ int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int
   int rc = bssn_host::device_sms(&sms);
   if (rc) return rc;
   const long long want = (npoints + amr::NTHREADS - 1) / amr::NTHREADS;
-  const long long cap_c = 5LL * 2 * sms, cap_p = 2LL * 2 * sms;  // two waves of resident CTAs
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  amr::fill_kernel<false><<<(int)(want < cap_c ? want : cap_c), amr::NTHREADS, 0, st>>>(pool, ops, nops, npoints, W);
+  const long long cap = 4LL * amr::MIN_CTAS * sms;  // four waves of resident CTAs
+  amr::fill_kernel<<<(int)(want < cap ? want : cap), amr::NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(
+      pool, ops, nops, npoints, W);
   cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return bssn_host::cuda_fail("fill launch", e);
-  amr::fill_kernel<true><<<(int)(want < cap_p ? want : cap_p), amr::NTHREADS, 0, st>>>(pool, ops, nops, npoints, W);
-  e = cudaGetLastError();
   if (e != cudaSuccess) return bssn_host::cuda_fail("fill launch", e);
   return 0;
 }
