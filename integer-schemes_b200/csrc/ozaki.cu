@@ -101,7 +101,10 @@ inline long long pass_tiles(const bssn_b200_block& b, const PassKind& k) {
 // smallest digit first; the outputs go out through shared memory so that the
 // stores are coalesced as well. The next tile's window is prefetched while a
 // tile is contracted.
-constexpr int FT = 256;       // threads of the fused kernel
+constexpr int FT = 512;       // threads of the fused kernel (16 warps)
+constexpr int QT = FT / 128;  // threads per line in the digit split
+constexpr int PPT = 32 / QT;  // window positions per thread
+constexpr int OPW = 16 / (FT / 128);  // outputs per thread in the recombination
 constexpr int FW = 33;        // float64 window pitch (conflict-free rows)
 constexpr int OP = 17;        // output staging pitch
 
@@ -133,6 +136,8 @@ struct FusedSmem {
   int8_t A[MAXK][LT * KW];
   double F[2][LT * FW];
   double O[3][LT * OP];
+  double mx[QT][LT];      // partial window maxima of the digit split
+  double K[2][LT * NO];   // KO sums of the earlier axes, prefetched with the window (ko_add passes)
   long long base[2][LT];  // first element of each line of the tile in F[buf]
 };
 
@@ -210,10 +215,16 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     long long lt = t, offset = 0;
     int s[3] = {a.one.sx, a.one.sy, a.one.sz}, core = 0;
     if (a.blocks) {
-      int lo = 0, hi = a.nblocks - 1;  // last block whose first tile is <= t
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (a.tile0[mid] <= t) lo = mid; else hi = mid - 1;
+      // last block whose first tile is <= t: a 32-way search by the warp
+      // (every thread of the CTA asks for the same t; tile0[0] = 0 <= t)
+      int lo = 0, n = a.nblocks;
+      while (n > 1) {
+        const int step = (n + 31) >> 5;
+        const int idx = lo + (tid & 31) * step;
+        const unsigned ok = __ballot_sync(0xffffffffu, idx < lo + n && a.tile0[idx] <= t);
+        const int last = 31 - __clz(ok);
+        lo += last * step;
+        n = min(step, n - last * step);
       }
       const bssn_b200_block* bk = a.blocks + lo;
       s[0] = bk->sx; s[1] = bk->sy; s[2] = bk->sz;
@@ -270,9 +281,22 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       q = q < 0 ? 0 : (q > ti.s_axis - 1 ? ti.s_axis - 1 : q);  // edge padding (derivatives.py:83-84)
       cp_async8(&sm.F[buf][r * FW + pos], src + sm.base[buf][r] + (long long)q * ti.stride);
     }
+    if (KOG && a.ko_add) {
+      // the KO sum this pass adds to, in the store loop's order
+      const double* kos = a.dst + ti.pbase * a.dst_slots + (long long)a.ko_slot * ti.n;
+      for (int i = tid; i < LT * NO; i += FT) {
+        const int rr = zaxis ? i / NO : i % LT;
+        const int o = zaxis ? i % NO : i / LT;
+        const long long l = ti.lb * LT + rr;
+        const int z = ti.z0 + o;
+        if (l < ti.nlines && z < ti.len)
+          cp_async8(&sm.K[buf][i], kos + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride);
+      }
+    }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
   };
   const long long ntiles = a.ntiles;
+  const double p7k = ldexp(1.0, 7 * a.k);  // 2^(7k): X is the window value scaled to 7k bits
   uint32_t phase = 0;
   bool failed = false;
   long long tile = blockIdx.x;
@@ -290,15 +314,19 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     __syncthreads();
     // ---- exponent and digits: threads r and r + 128 take the two 16-position halves of line r ----
-    const int r = tid & (LT - 1), half = tid >> 7;
-    const double* Fr = &sm.F[buf][r * FW];
-    double m0 = 0.0, m1 = 0.0;
+    const int r = tid & (LT - 1), q4 = tid >> 7;
+    const double* Fr = &sm.F[buf][r * FW + PPT * q4];
+    {
+      double m0 = 0.0;
 #pragma unroll
-    for (int pos = 0; pos < KWL; pos += 2) {
-      m0 = fmax(m0, fabs(Fr[pos]));
-      m1 = fmax(m1, fabs(Fr[pos + 1]));
+      for (int j = 0; j < PPT; ++j)
+        if (PPT * q4 + j < KWL) m0 = fmax(m0, fabs(Fr[j]));
+      sm.mx[q4][r] = m0;
     }
-    const double m = fmax(m0, m1);
+    __syncthreads();
+    double m = sm.mx[0][r];
+#pragma unroll
+    for (int q = 1; q < QT; ++q) m = fmax(m, sm.mx[q][r]);
     int e = 0;
     if (m > 0.0) {
       int ex;
@@ -308,29 +336,24 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     const double sc = ldexp(1.0, e);
     const double isc = ldexp(1.0, -e);  // scaling by a power of two is exact
     {
-      uint32_t wd[MAXK][4];
+      // X = rint(f 2^(7k - e)), |X| <= 2^(7k-1); two's complement gives
+      // X = top 2^(7(k-1)) + sum_j d_j 2^(7j), 0 <= d_j < 128, |top| <= 64
+      long long X[PPT];
 #pragma unroll
-      for (int s2 = 0; s2 < MAXK; ++s2) wd[s2][0] = wd[s2][1] = wd[s2][2] = wd[s2][3] = 0u;
+      for (int j = 0; j < PPT; ++j) X[j] = PPT * q4 + j < KWL ? __double2ll_rn((Fr[j] * isc) * p7k) : 0;
+      int8_t* dst = &sm.A[0][canon(r, PPT * q4, LT)];
+      for (int s2 = 0; s2 < a.k; ++s2, dst += LT * KW) {  // plane by plane, most significant first
+        const int sh = 7 * (a.k - 1 - s2);
+        const uint32_t mask = s2 == 0 ? 255u : 127u;
+        uint32_t w0 = 0u, w1 = 0u;
 #pragma unroll
-      const double p7k = ldexp(1.0, 7 * a.k);
-      for (int j = 0; j < 16; ++j) {
-        const int pos = 16 * half + j;
-        // X = rint(f 2^(7k - e)), |X| <= 2^(7k-1); two's complement gives
-        // X = top 2^(7(k-1)) + sum_j d_j 2^(7j), 0 <= d_j < 128, |top| <= 64
-        const long long X = pos < KWL ? __double2ll_rn((Fr[pos] * isc) * p7k) : 0;
-#pragma unroll
-        for (int s2 = 0; s2 < MAXK; ++s2) {
-          if (s2 < a.k) {
-            const long long sh = X >> (7 * (a.k - 1 - s2));
-            const int d = s2 == 0 ? (int)sh : (int)(sh & 127);
-            wd[s2][j >> 2] |= (uint32_t)(d & 255) << (8 * (j & 3));
-          }
+        for (int j = 0; j < PPT; ++j) {
+          const uint32_t d = (uint32_t)(X[j] >> sh) & mask;
+          if (j < 4) w0 |= d << (8 * j);
+          else w1 |= d << (8 * (j - 4));
         }
+        *reinterpret_cast<uint2*>(dst) = make_uint2(w0, w1);
       }
-#pragma unroll
-      for (int s2 = 0; s2 < MAXK; ++s2)
-        if (s2 < a.k)
-          *reinterpret_cast<uint4*>(&sm.A[s2][canon(r, 16 * half, LT)]) = make_uint4(wd[s2][0], wd[s2][1], wd[s2][2], wd[s2][3]);
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
@@ -366,26 +389,25 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     }
     phase ^= 1u;
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // ---- recombine: warp w reads TMEM lanes 32 (w % 4).., outputs 8 (w / 4).. ----
+    // ---- recombine: warp w reads TMEM lanes 32 (w % 4).., outputs OPW (w / 4).. ----
     const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
-    const int oc = 8 * (warp >> 2);
-    double r1[8], r2[8], rk[8];
+    const int oc = OPW * (warp >> 2);
+    double r1[OPW], r2[OPW], rk[OPW];
 #pragma unroll
-    for (int o = 0; o < 8; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
+    for (int o = 0; o < OPW; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
     double w = ldexp(1.0, -7 * a.k);  // weight of the smallest digit plane
     for (int s2 = a.k - 1; s2 >= 0; --s2, w *= 128.0) {
-      uint32_t v[NG][8];
+      uint32_t v[NG][OPW];
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         const uint32_t addr = tmem + lane + (uint32_t)(NC * s2 + NO * g + oc);
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
-                     : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3]), "=r"(v[g][4]),
-                       "=r"(v[g][5]), "=r"(v[g][6]), "=r"(v[g][7])
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                     : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3])
                      : "r"(addr));
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-      for (int o = 0; o < 8; ++o) {
+      for (int o = 0; o < OPW; ++o) {
         r1[o] += (double)(int)v[0][o] * w;
         if (D2) r2[o] += (double)((int)v[D2 ? 1 : 0][o] * 128 + (int)v[D2 ? 2 : 0][o]) * w;
         if (KOG) rk[o] += (double)(int)v[KOG ? GKO : 0][o] * w;
@@ -394,7 +416,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     // the recombining thread's line is r too (TMEM lane = line): its exponent is sc
 #pragma unroll
-    for (int o = 0; o < 8; ++o) {
+    for (int o = 0; o < OPW; ++o) {
       sm.O[0][r * OP + oc + o] = (r1[o] * sc) * w1;
       if (D2) sm.O[1][r * OP + oc + o] = (r2[o] * sc) * w2;
       if (KOG) sm.O[2][r * OP + oc + o] = (rk[o] * sc) * wko;
@@ -410,10 +432,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
         double* out = a.dst + ti.pbase * a.dst_slots + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride;
         out[(long long)a.d1_slot * ti.n] = sm.O[0][rr * OP + o];
         if (D2) out[(long long)a.d2_slot * ti.n] = sm.O[1][rr * OP + o];
-        if (KOG) {
-          double* kp = out + (long long)a.ko_slot * ti.n;
-          *kp = a.ko_add ? *kp + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
-        }
+        if (KOG) out[(long long)a.ko_slot * ti.n] = a.ko_add ? sm.K[buf][i] + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
       }
     }
     __syncthreads();  // TMEM columns, digits and output staging are reused by the next tile
