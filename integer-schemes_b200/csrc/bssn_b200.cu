@@ -861,7 +861,6 @@ __global__ void __launch_bounds__(128) stage_derivs_kernel(
     const double* __restrict__ D, int nslot, const double* __restrict__ S, int stage, int ko_slots,
     double chi_floor, double alpha_floor, const bssn_b200_block* __restrict__ blocks, int nblocks,
     const long long* __restrict__ pts0, long long npoints) {
-  __shared__ double sd[2][10][128];  // [buffer][d1 x3, d2 x6, KO][thread]
   const Params P0 = load_params(S);
   const double cs = stage == 0 ? 0.0 : (stage == 3 ? 1.0 : 0.5);
   const double dt = P0.dt;
@@ -887,39 +886,17 @@ __global__ void __launch_bounds__(128) stage_derivs_kernel(
     P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
     P.t = P0.t + cs * P0.dt;  // stage time t, t+dt/2, t+dt/2, t+dt (evolve.py:125-131)
     auto fld = [&](int k) -> double { return __ldg(Y + gidx + (long long)k * n); };
-    // each thread copies its own point's derivatives of the next field in
-    // stream order into its own shared-memory column while it consumes the
-    // current field's: the slot loads stay in flight behind the algebra
-    auto issue = [&](auto fc, int b) {
-      constexpr int g = decltype(fc)::value;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) cp_async8(&sd[b][a][threadIdx.x], Dq + (long long)d1slot(g, a) * n);
-      if (has_d2(g)) {
-#pragma unroll
-        for (int pp = 0; pp < 6; ++pp) cp_async8(&sd[b][3 + pp][threadIdx.x], Dq + (long long)d2slot(g, pp) * n);
-      }
-      if (ko_slots) cp_async8(&sd[b][9][threadIdx.x], Dq + (long long)(138 + g) * n);
-      cp_async_commit();
-    };
-    issue(std::integral_constant<int, stream_field(0)>{}, 0);
+    auto drv = [&](int s) -> double { return __ldg(Dq + (long long)s * n); };
     Stream<true, false> acc;
     acc.init(fld);
     Unroll<0, NFIELD>::run([&](auto ic) {
-      constexpr int idx = decltype(ic)::value;
-      constexpr int f = stream_field(idx);
-      constexpr int b = idx & 1;
-      if (idx + 1 < NFIELD) {
-        issue(std::integral_constant<int, stream_field(idx + 1 < NFIELD ? idx + 1 : idx)>{}, b ^ 1);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
-      }
+      constexpr int f = stream_field(decltype(ic)::value);
       double d1[3], d2[6];
 #pragma unroll
-      for (int a = 0; a < 3; ++a) d1[a] = sd[b][a][threadIdx.x];
+      for (int a = 0; a < 3; ++a) d1[a] = drv(d1slot(f, a));
 #pragma unroll
-      for (int pp = 0; pp < 6; ++pp) d2[pp] = has_d2(f) ? sd[b][3 + pp][threadIdx.x] : 0.0;
-      acc.consume(f, d1, d2, ko_slots ? sd[b][9][threadIdx.x] : 0.0, P, fld);
+      for (int pp = 0; pp < 6; ++pp) d2[pp] = has_d2(f) ? drv(d2slot(f, pp)) : 0.0;
+      acc.consume(f, d1, d2, ko_slots ? drv(138 + f) : 0.0, P, fld);
     });
     double* A = ACC + gidx;
     double* O = OUT + gidx;
