@@ -541,6 +541,24 @@ def bench_amr(args):
     finite = bool(torch.isfinite(U_g).all().item())
     interior = pool.interior_points
     value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
+    # where a stage's time goes, timed alone after the timed region (CUDA events)
+    def ev_ms(fn, reps=5):
+        fn()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return round(a.elapsed_time(b) / reps, 3)
+    bufs = evo.buffers(U_g)
+    Y_t = U_g.clone()
+    breakdown = {"fill_ms_per_stage": ev_ms(lambda: evo.fill(Y_t)) if evo.dplan is not None else 0.0,
+                 "stage_ms": ev_ms(lambda: evo.stage(1, U_g, Y_t, bufs["ACC"], bufs["Yb"], S_g))}
+    if oz_k:
+        breakdown["derivative_bundle_ms"] = ev_ms(lambda: evo.derivatives(Y_t, S_g))
+    del Y_t
     fills = len(evo.dplan.fill) if evo.dplan is not None else 0
     ghost_counts = evo.plan.counts if evo.plan is not None else None
     variant = evo.variant
@@ -591,7 +609,7 @@ def bench_amr(args):
                    "autotune_ms": {str(k): v for k, v in tune.items()},
                    "plan_s": round(t_plan, 2), "parallelism": f"replicas x{world}"},
         "clocks": clk, "gpu_launches": (4 * per_stage + 1) * args.steps, "finite": finite,
-        "ghost_points": ghost_counts,
+        "ghost_points": ghost_counts, "breakdown": breakdown,
         "constraints": tracked, "roofline": None, "e2e": None, "cpu_baseline": None,
     }
     if oz_k:
