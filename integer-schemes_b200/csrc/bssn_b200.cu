@@ -866,13 +866,23 @@ __global__ void __launch_bounds__(128) stage_derivs_kernel(
   const double dt = P0.dt;
   const double hstep = (stage == 2) ? dt : 0.5 * dt;
   const double w6 = dt / 6.0;
-  for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < npoints;
-       q += (long long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = nblocks - 1;  // last block whose first point is <= q
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (pts0[mid] <= q) lo = mid; else hi = mid - 1;
+  const int lane = threadIdx.x & 31;
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  // warps walk the points together (q0 is the warp's first point), so the
+  // block lookup is one 32-way search per warp instead of one per point
+  for (long long q0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); q0 < npoints; q0 += stride) {
+    const long long q = q0 + lane;
+    int lo = 0, nb = nblocks;  // last block whose first point is <= q0 (pts0[0] = 0)
+    while (nb > 1) {
+      const int step = (nb + 31) >> 5;
+      const int idx = lo + lane * step;
+      const unsigned ok = __ballot_sync(0xffffffffu, idx < lo + nb && pts0[idx] <= q0);
+      const int last = 31 - __clz(ok);
+      lo += last * step;
+      nb = min(step, nb - last * step);
     }
+    while (lo + 1 < nblocks && pts0[lo + 1] <= q) ++lo;  // a warp that straddles blocks
+    if (q >= npoints) continue;
     const bssn_b200_block bk = blocks[lo];
     const int c = bk.core;
     const int ey = bk.sy - 2 * c, ez = bk.sz - 2 * c;
