@@ -40,7 +40,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "BSSN RHS Mpoint-updates/s (RK4 step, fused FP64)"
 UNIT = "Mpoint-updates/s"
-FLOPS_PER_POINT = 6840      # algorithmic FP64 flops per RHS point-update
+FLOPS_PER_POINT = 6714      # algorithmic FP64 flops per RHS point-update (oracle/count_flops.py): algebra 4,278 + derivatives 2,436
 KO_FLOPS_PER_POINT = 936    # 24 fields x 3 axes x (7 taps: 7 mul + 6 add)
 STAGE_BYTES = 960           # read Y, U, ACC; write ACC, Y_next (5 x 24 x 8 B)
 # DRAM bytes per point of one stage launch, dram__bytes_read.sum + dram__bytes_write.sum

@@ -265,14 +265,20 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   // its edge padding; tail lines repeat the last line); the lines' first
   // elements (block-local, axis coordinate 0) are tabled once per tile.
   // Callers place it right after a barrier.
-  auto load_window = [&](const TileInfo& ti, int buf) {
+  // The first four warps look the tile up (the base table needs 128
+  // threads) and thread 0 publishes it in sti[buf] for the other warps.
+  __shared__ TileInfo sti[2];
+  auto load_window = [&](long long t, int buf) {
     if (tid < LT) {
-      int l = (int)ti.lb * LT + tid;  // lines of a block stay below 2^31
-      if (l >= ti.nlines) l = (int)ti.nlines - 1;
-      const int slow = l / ti.e_fast, fast = l % ti.e_fast;
-      sm.base[buf][tid] = (long long)(slow + ti.m_slow) * ti.st_slow + (long long)(fast + ti.m_fast) * ti.st_fast;
+      const TileInfo tw = tile_info(t);
+      int l = (int)tw.lb * LT + tid;  // lines of a block stay below 2^31
+      if (l >= tw.nlines) l = (int)tw.nlines - 1;
+      const int slow = l / tw.e_fast, fast = l % tw.e_fast;
+      sm.base[buf][tid] = (long long)(slow + tw.m_slow) * tw.st_slow + (long long)(fast + tw.m_fast) * tw.st_fast;
+      if (tid == 0) sti[buf] = tw;
     }
     __syncthreads();
+    const TileInfo ti = sti[buf];
     const double* src = a.src + ti.pbase * a.src_slots + (long long)a.src_slot * ti.n;
     for (int i = tid; i < LT * KWL; i += FT) {
       const int r = zaxis ? i / KWL : i % LT;
@@ -300,14 +306,10 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   uint32_t phase = 0;
   bool failed = false;
   long long tile = blockIdx.x;
-  TileInfo next{};
-  if (tile < ntiles) {
-    next = tile_info(tile);
-    load_window(next, 0);
-  }
+  if (tile < ntiles) load_window(tile, 0);
   int buf = 0;
   for (; tile < ntiles && !failed; tile += gridDim.x, buf ^= 1) {
-    const TileInfo ti = next;
+    const TileInfo ti = sti[buf];  // published by the load of this tile's window
     const double w1 = (1.0 / 60.0) * (1.0 / ti.h);
     const double w2 = (1.0 / 180.0) * (1.0 / (ti.h * ti.h));
     const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / ti.h);
@@ -358,10 +360,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
     // ---- prefetch the next tile's window; thread 0 issues the contractions ----
-    if (tile + gridDim.x < ntiles) {
-      next = tile_info(tile + gridDim.x);
-      load_window(next, buf ^ 1);
-    }
+    if (tile + gridDim.x < ntiles) load_window(tile + gridDim.x, buf ^ 1);
     if (tid == 0) {
       const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
       for (int s2 = 0; s2 < a.k; ++s2) {
