@@ -394,12 +394,39 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     double r1[OPW], r2[OPW], rk[OPW];
 #pragma unroll
     for (int o = 0; o < OPW; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
+    // planes in pairs from the smallest: (q_{s-1} 128 + q_s) is an exact
+    // int32 (|C2 pair| < 2^25), converted once and added with the weight of
+    // plane s; an odd top plane goes alone
     double w = ldexp(1.0, -7 * a.k);  // weight of the smallest digit plane
-    for (int s2 = a.k - 1; s2 >= 0; --s2, w *= 128.0) {
+    int s2 = a.k - 1;
+    for (; s2 >= 1; s2 -= 2, w *= 16384.0) {
+      uint32_t v[2][NG][OPW];  // [0]: plane s2 - 1 (weight 128 w), [1]: plane s2
+#pragma unroll
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int g = 0; g < NG; ++g) {
+          const uint32_t addr = tmem + lane + (uint32_t)(NC * (s2 - 1 + h) + NO * g + oc);
+          asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                       : "=r"(v[h][g][0]), "=r"(v[h][g][1]), "=r"(v[h][g][2]), "=r"(v[h][g][3])
+                       : "r"(addr));
+        }
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+      for (int o = 0; o < OPW; ++o) {
+        r1[o] += (double)((int)v[0][0][o] * 128 + (int)v[1][0][o]) * w;
+        if (D2) {
+          const int c2a = (int)v[0][D2 ? 1 : 0][o] * 128 + (int)v[0][D2 ? 2 : 0][o];
+          const int c2b = (int)v[1][D2 ? 1 : 0][o] * 128 + (int)v[1][D2 ? 2 : 0][o];
+          r2[o] += (double)(c2a * 128 + c2b) * w;
+        }
+        if (KOG) rk[o] += (double)((int)v[0][KOG ? GKO : 0][o] * 128 + (int)v[1][KOG ? GKO : 0][o]) * w;
+      }
+    }
+    if (s2 == 0) {
       uint32_t v[NG][OPW];
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
-        const uint32_t addr = tmem + lane + (uint32_t)(NC * s2 + NO * g + oc);
+        const uint32_t addr = tmem + lane + (uint32_t)(NO * g + oc);
         asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
                      : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3])
                      : "r"(addr));

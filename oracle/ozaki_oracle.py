@@ -19,8 +19,9 @@ computes, so that the GPU result can be compared bit for bit:
 * per plane the exact integer stencil sums C1, C2 (as 2·128 + 14 / −4·128 + 22
   high and low digits) and KO6/KO8 (the banded integer design of the
   reference's MCS Ozaki derivative, 2D/src/mcs2d/schemes/ozaki.py:286-323);
-* recombination in float64, smallest plane first, r += acc · 2^(-7(s+1))
-  (exact products, one rounding per add), then (r · 2^e) · w with
+* recombination in float64, planes in pairs from the smallest,
+  r += (acc_{s-1}·128 + acc_s) · 2^(-7(s+1)) (exact integer pairs and
+  products, one rounding per add; an odd top plane alone), then (r · 2^e) · w with
   w = (1/60)(1/h), (1/180)(1/h²), (1/64 or 1/256)(σ/h);
 * the bundle runs the passes of derivative_bundle.py:31-48 — per field the
   x, y, z passes (KO summed x, then y, then z), then the mixed second
@@ -72,12 +73,17 @@ def _band(digits: np.ndarray, coef: np.ndarray, R: int) -> np.ndarray:
 
 
 def _recombine(acc: np.ndarray, k: int) -> np.ndarray:
-    """sum over planes, smallest first: r = r + acc_s 2^(-7(s+1)) in float64."""
+    """Planes in pairs from the smallest, r = r + (acc_{s-1} 128 + acc_s) 2^(-7(s+1))
+    in float64 (the pair is an exact integer), an odd top plane alone."""
     r = np.zeros(acc.shape[1:], dtype=np.float64)
     w = math.ldexp(1.0, -7 * k)
-    for s in range(k - 1, -1, -1):
-        r = r + acc[s].astype(np.float64) * w
-        w *= 128.0
+    s = k - 1
+    while s >= 1:
+        r = r + (acc[s - 1] * 128 + acc[s]).astype(np.float64) * w
+        w *= 16384.0
+        s -= 2
+    if s == 0:
+        r = r + acc[0].astype(np.float64) * w
     return r
 
 
