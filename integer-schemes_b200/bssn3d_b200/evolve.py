@@ -252,20 +252,26 @@ class HostStepPipeline:
     copies overlapped with the compute: while step i runs on the device, the
     state of step i+1 is copied in and the result of step i-1 is copied out.
 
-    Two device slots, each with its own captured step graph (the stage
-    buffers are shared: the steps themselves run one after another on the
-    compute stream), and three streams (copy in, compute, copy out) ordered
-    by events. For pinned host tensors the throughput approaches the device
-    step rate once the two copies of a state take less time than its step.
+    ``nslots`` device slots (default 3), each with its own captured step
+    graph (the stage buffers are shared: the steps themselves run one after
+    another on the compute stream), and three streams (copy in, compute, copy
+    out) ordered by events. A slot is refilled only after its previous result
+    is out, so with two slots a step waits for the copy out and the copy in
+    of its slot back to back; a third slot hides both behind the compute of
+    the steps between. For pinned host tensors the throughput approaches the
+    device step rate once each copy of a state takes less time than a step.
     Every item is advanced from the same start time ``t``.
     """
 
-    def __init__(self, evo: BSSNEvolution, shape, dt: float, t: float = 0.0, device="cuda"):
+    def __init__(self, evo: BSSNEvolution, shape, dt: float, t: float = 0.0, device="cuda", nslots: int = 3):
         self.evo = evo
         self.device = torch.device(device)
         S = evo._S(t, dt, self.device)
+        self.nslots = int(nslots)
+        if self.nslots < 1:
+            raise ValueError("nslots must be >= 1")
         self.slots = []
-        for _ in range(2):
+        for _ in range(self.nslots):
             U = torch.empty(tuple(shape), dtype=torch.float64, device=self.device)
             U.zero_()
             U[0].fill_(1.0)     # a harmless state for the capture's warm-up step
@@ -276,9 +282,9 @@ class HostStepPipeline:
         self.s_in = torch.cuda.Stream(self.device)
         self.s_comp = torch.cuda.Stream(self.device)
         self.s_out = torch.cuda.Stream(self.device)
-        self.ev_in = [torch.cuda.Event() for _ in range(2)]
-        self.ev_comp = [torch.cuda.Event() for _ in range(2)]
-        self.ev_out = [torch.cuda.Event() for _ in range(2)]
+        self.ev_in = [torch.cuda.Event() for _ in range(self.nslots)]
+        self.ev_comp = [torch.cuda.Event() for _ in range(self.nslots)]
+        self.ev_out = [torch.cuda.Event() for _ in range(self.nslots)]
 
     def _capture(self, U, S):
         evo = self.evo
@@ -305,9 +311,9 @@ class HostStepPipeline:
         for st in (self.s_in, self.s_comp, self.s_out):
             st.wait_stream(cur)
         for i, (hin, hout) in enumerate(zip(host_in, host_out)):
-            k = i & 1
+            k = i % self.nslots
             g, U = self.slots[k]
-            if i >= 2:
+            if i >= self.nslots:
                 self.s_in.wait_event(self.ev_out[k])      # slot k's previous result is out
             with torch.cuda.stream(self.s_in):
                 U.copy_(hin, non_blocking=True)

@@ -141,6 +141,18 @@ struct FusedSmem {
   long long base[2][LT];  // first element of each line of the tile in F[buf]
 };
 
+// Exact conversions between float64 and integers below 2^51 on the float64
+// and integer pipes: adding 1.5 * 2^52 puts rint(v) in the low mantissa bits
+// (round to nearest even, like cvt.rni), and the reverse undoes it.
+constexpr double MAGIC = 6755399441055744.0;  // 1.5 * 2^52
+constexpr long long MAGIC_BITS = 0x4338000000000000LL;
+__device__ __forceinline__ long long rint_to_ll(double v) {  // |v| < 2^51
+  return __double_as_longlong(__dadd_rn(v, MAGIC)) - MAGIC_BITS;
+}
+__device__ __forceinline__ double ll_to_double(long long n) {  // |n| < 2^51
+  return __dsub_rn(__longlong_as_double(n + MAGIC_BITS), MAGIC);
+}
+
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -329,20 +341,40 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     double m = sm.mx[0][r];
 #pragma unroll
     for (int q = 1; q < QT; ++q) m = fmax(m, sm.mx[q][r]);
+    // e = frexp(m) + 1 so that |f| 2^-e < 1/2; sc = 2^e, isc = 2^-e (exact).
+    // A normal m reads its exponent field; subnormal and huge windows take
+    // the library calls.
     int e = 0;
+    double sc = 1.0, isc = 1.0;
     if (m > 0.0) {
-      int ex;
-      frexp(m, &ex);  // m = fr * 2^ex, fr in [0.5, 1)
-      e = ex + 1;     // |f| 2^-e < 1/2
+      const int bexp = (int)((__double_as_longlong(m) >> 52) & 0x7ff);
+      if (bexp > 0 && bexp < 2044) {  // e in [-1020, 1022]: both powers are normal
+        e = bexp - 1022 + 1;
+        sc = __longlong_as_double((long long)(e + 1023) << 52);
+        isc = __longlong_as_double((long long)(1023 - e) << 52);
+      } else {
+        int ex;
+        frexp(m, &ex);  // m = fr * 2^ex, fr in [0.5, 1)
+        e = ex + 1;
+        sc = ldexp(1.0, e);
+        isc = ldexp(1.0, -e);
+      }
     }
-    const double sc = ldexp(1.0, e);
-    const double isc = ldexp(1.0, -e);  // scaling by a power of two is exact
     {
       // X = rint(f 2^(7k - e)), |X| <= 2^(7k-1); two's complement gives
       // X = top 2^(7(k-1)) + sum_j d_j 2^(7j), 0 <= d_j < 128, |top| <= 64
       long long X[PPT];
 #pragma unroll
-      for (int j = 0; j < PPT; ++j) X[j] = PPT * q4 + j < KWL ? __double2ll_rn((Fr[j] * isc) * p7k) : 0;
+      for (int j = 0; j < PPT; ++j) X[j] = 0;
+      if (a.k <= 7) {  // |v| <= 2^48: the float64-pipe rounding
+#pragma unroll
+        for (int j = 0; j < PPT; ++j)
+          if (PPT * q4 + j < KWL) X[j] = rint_to_ll((Fr[j] * isc) * p7k);  // exact power-of-two scaling
+      } else {
+#pragma unroll
+        for (int j = 0; j < PPT; ++j)
+          if (PPT * q4 + j < KWL) X[j] = __double2ll_rn((Fr[j] * isc) * p7k);
+      }
       int8_t* dst = &sm.A[0][canon(r, PPT * q4, LT)];
       for (int s2 = 0; s2 < a.k; ++s2, dst += LT * KW) {  // plane by plane, most significant first
         const int sh = 7 * (a.k - 1 - s2);
@@ -413,13 +445,13 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
       for (int o = 0; o < OPW; ++o) {
-        r1[o] += (double)((int)v[0][0][o] * 128 + (int)v[1][0][o]) * w;
+        r1[o] += ll_to_double((int)v[0][0][o] * 128 + (int)v[1][0][o]) * w;
         if (D2) {
           const int c2a = (int)v[0][D2 ? 1 : 0][o] * 128 + (int)v[0][D2 ? 2 : 0][o];
           const int c2b = (int)v[1][D2 ? 1 : 0][o] * 128 + (int)v[1][D2 ? 2 : 0][o];
-          r2[o] += (double)(c2a * 128 + c2b) * w;
+          r2[o] += ll_to_double(c2a * 128 + c2b) * w;
         }
-        if (KOG) rk[o] += (double)((int)v[0][KOG ? GKO : 0][o] * 128 + (int)v[1][KOG ? GKO : 0][o]) * w;
+        if (KOG) rk[o] += ll_to_double((int)v[0][KOG ? GKO : 0][o] * 128 + (int)v[1][KOG ? GKO : 0][o]) * w;
       }
     }
     if (s2 == 0) {

@@ -9,7 +9,8 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def test_pipelined_host_steps_equal_single_steps():
+@pytest.mark.parametrize("nslots", [1, 2, 3])
+def test_pipelined_host_steps_equal_single_steps(nslots):
     from bssn3d_b200 import initial_data as ID
     from bssn3d_b200.evolve import BSSNEvolution, HostStepPipeline
     from bssn3d_b200.state import BSSNState
@@ -19,7 +20,7 @@ def test_pipelined_host_steps_equal_single_steps():
     states = [U + 1e-4 * rng.standard_normal(U.shape) * (k > 0) for k in range(5)]
     host_in = [torch.from_numpy(s).pin_memory() for s in states]
     host_out = [torch.empty_like(h).pin_memory() for h in host_in]
-    pipe = HostStepPipeline(evo, U.shape, dt, 0.3)
+    pipe = HostStepPipeline(evo, U.shape, dt, 0.3, nslots=nslots)
     pipe.run(host_in, host_out)
     torch.cuda.synchronize()
     for s, h in zip(states, host_out):
