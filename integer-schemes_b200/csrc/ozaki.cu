@@ -136,7 +136,6 @@ struct FusedSmem {
   int8_t A[MAXK][LT * KW];
   double F[2][LT * FW];
   double O[3][LT * OP];
-  double mx[QT][LT];      // partial window maxima of the digit split
   double K[2][LT * NO];   // KO sums of the earlier axes, prefetched with the window (ko_add passes)
   long long base[2][LT];  // first element of each line of the tile in F[buf]
 };
@@ -277,10 +276,11 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   // its edge padding; tail lines repeat the last line); the lines' first
   // elements (block-local, axis coordinate 0) are tabled once per tile.
   // Callers place it right after a barrier.
-  // The first four warps look the tile up (the base table needs 128
-  // threads) and thread 0 publishes it in sti[buf] for the other warps.
+  // The first four warps look tile t up (the base table needs 128 threads)
+  // and thread 0 publishes it in sti[buf]; a barrier must follow before
+  // issue_window reads them.
   __shared__ TileInfo sti[2];
-  auto load_window = [&](long long t, int buf) {
+  auto lookup = [&](long long t, int buf) {
     if (tid < LT) {
       const TileInfo tw = tile_info(t);
       int l = (int)tw.lb * LT + tid;  // lines of a block stay below 2^31
@@ -289,7 +289,8 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       sm.base[buf][tid] = (long long)(slow + tw.m_slow) * tw.st_slow + (long long)(fast + tw.m_fast) * tw.st_fast;
       if (tid == 0) sti[buf] = tw;
     }
-    __syncthreads();
+  };
+  auto issue_window = [&](int buf) {
     const TileInfo ti = sti[buf];
     const double* src = a.src + ti.pbase * a.src_slots + (long long)a.src_slot * ti.n;
     for (int i = tid; i < LT * KWL; i += FT) {
@@ -318,29 +319,35 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   uint32_t phase = 0;
   bool failed = false;
   long long tile = blockIdx.x;
-  if (tile < ntiles) load_window(tile, 0);
+  if (tile < ntiles) {
+    lookup(tile, 0);
+    __syncthreads();
+    issue_window(0);
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
+  }
   int buf = 0;
   for (; tile < ntiles && !failed; tile += gridDim.x, buf ^= 1) {
     const TileInfo ti = sti[buf];  // published by the load of this tile's window
     const double w1 = (1.0 / 60.0) * (1.0 / ti.h);
     const double w2 = (1.0 / 180.0) * (1.0 / (ti.h * ti.h));
     const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / ti.h);
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    __syncthreads();
-    // ---- exponent and digits: threads r and r + 128 take the two 16-position halves of line r ----
+    // (this tile's window has landed: the barrier that ended the previous
+    // tile, or the prologue's, followed every thread's wait for its copies)
+    // ---- exponent and digits: the four threads of line r take 8 positions each ----
     const int r = tid & (LT - 1), q4 = tid >> 7;
     const double* Fr = &sm.F[buf][r * FW + PPT * q4];
+    double m = 0.0;
     {
-      double m0 = 0.0;
+      const double* Fl = &sm.F[buf][r * FW];  // every thread of the line takes the whole window's max
+      double m0 = 0.0, m1 = 0.0;
 #pragma unroll
-      for (int j = 0; j < PPT; ++j)
-        if (PPT * q4 + j < KWL) m0 = fmax(m0, fabs(Fr[j]));
-      sm.mx[q4][r] = m0;
+      for (int pos = 0; pos < KWL; pos += 2) {
+        m0 = fmax(m0, fabs(Fl[pos]));
+        m1 = fmax(m1, fabs(Fl[pos + 1]));
+      }
+      m = fmax(m0, m1);
     }
-    __syncthreads();
-    double m = sm.mx[0][r];
-#pragma unroll
-    for (int q = 1; q < QT; ++q) m = fmax(m, sm.mx[q][r]);
     // e = frexp(m) + 1 so that |f| 2^-e < 1/2; sc = 2^e, isc = 2^-e (exact).
     // A normal m reads its exponent field; subnormal and huge windows take
     // the library calls.
@@ -390,9 +397,10 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    const bool more = tile + gridDim.x < ntiles;
+    if (more) lookup(tile + gridDim.x, buf ^ 1);  // its base table and sti slot were last read last tile
     __syncthreads();
-    // ---- prefetch the next tile's window; thread 0 issues the contractions ----
-    if (tile + gridDim.x < ntiles) load_window(tile + gridDim.x, buf ^ 1);
+    // ---- thread 0 issues the contractions; everyone prefetches the next tile's window ----
     if (tid == 0) {
       const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
       for (int s2 = 0; s2 < a.k; ++s2) {
@@ -406,6 +414,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
                        smem_u32(&mbar))
                    : "memory");
     }
+    if (more) issue_window(buf ^ 1);
     uint32_t done = 0;
     for (long long it = 0; it < WAIT_LIMIT && !done; ++it) {
       asm volatile(
@@ -493,7 +502,10 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
         if (KOG) out[(long long)a.ko_slot * ti.n] = a.ko_add ? sm.K[buf][i] + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
       }
     }
-    __syncthreads();  // TMEM columns, digits and output staging are reused by the next tile
+    // the next tile's window (this thread's copies) has landed; the barrier
+    // publishes it and frees TMEM columns, digits and output staging
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    __syncthreads();
   }
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
