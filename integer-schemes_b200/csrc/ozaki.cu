@@ -397,10 +397,11 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    const bool more = tile + gridDim.x < ntiles;
-    if (more) lookup(tile + gridDim.x, buf ^ 1);  // its base table and sti slot were last read last tile
     __syncthreads();
-    // ---- thread 0 issues the contractions; everyone prefetches the next tile's window ----
+    // ---- thread 0 issues the contractions; while they run, the first four warps
+    // look the next tile up (its base table and sti slot were last read last
+    // tile); the barrier after the wait publishes it and everyone prefetches
+    // the next tile's window behind the recombination and stores ----
     if (tid == 0) {
       const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
       for (int s2 = 0; s2 < a.k; ++s2) {
@@ -414,7 +415,8 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
                        smem_u32(&mbar))
                    : "memory");
     }
-    if (more) issue_window(buf ^ 1);
+    const bool more = tile + gridDim.x < ntiles;
+    if (more) lookup(tile + gridDim.x, buf ^ 1);
     uint32_t done = 0;
     for (long long it = 0; it < WAIT_LIMIT && !done; ++it) {
       asm volatile(
@@ -428,6 +430,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       failed = true;
     }
     phase ^= 1u;
+    if (more && !failed) issue_window(buf ^ 1);
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     // ---- recombine: warp w reads TMEM lanes 32 (w % 4).., outputs OPW (w / 4).. ----
     const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
