@@ -95,17 +95,27 @@ inline long long pass_tiles(const bssn_b200_block& b, const PassKind& k) {
 // edge-clamped) lands in shared memory by cp.async, laid out so that the
 // copies are coalesced (line-contiguous windows for the z axis, line-
 // interleaved for x and y); each line gets one power-of-two exponent for its
-// window and two threads per line write its k digit planes straight into the
-// canonical operand layout; thread 0 issues the k contractions; the two
-// warpgroups read 8 outputs each back from TMEM and recombine them
-// smallest digit first; the outputs go out through shared memory so that the
-// stores are coalesced as well. The next tile's window is prefetched while a
-// tile is contracted.
-constexpr int FT = 512;       // threads of the fused kernel (16 warps)
-constexpr int QT = FT / 128;  // threads per line in the digit split
-constexpr int PPT = 32 / QT;  // window positions per thread
-constexpr int OPW = 16 / (FT / 128);  // outputs per thread in the recombination
-constexpr int FW = 33;        // float64 window pitch (conflict-free rows)
+// window and its threads write its k digit planes straight into the
+// canonical operand layout; thread 0 issues the k contractions; the warps
+// read the outputs back from TMEM and recombine them smallest digit first;
+// the outputs go out through shared memory so that the stores are coalesced
+// as well. The next tile's window is prefetched while a tile is contracted.
+//
+// Two shapes: passes with second derivatives (N = 48 or 64: all 512 TMEM
+// columns for k = 6..8) run one 512-thread CTA per SM; the others (N = 16 or
+// 32: at most 256 columns) run two 256-thread CTAs per SM in ~106 KB of
+// shared memory each (output staging inside the spent window buffer, KO sums
+// read back from global memory), so that one CTA's barriers overlap the
+// other's work.
+template <bool SMALL>
+struct Cfg {
+  static constexpr int FT = SMALL ? 256 : 512;  // threads
+  static constexpr int QT = FT / 128;            // threads per line in the digit split
+  static constexpr int PPT = 32 / QT;            // window positions per thread
+  static constexpr int OPW = 16 / QT;            // outputs per thread in the recombination
+  static constexpr int FW = SMALL ? 35 : 33;     // float64 window pitch (conflict-free rows; 35 also holds the staging)
+  static constexpr int CTAS = SMALL ? 2 : 1;     // CTAs per SM
+};
 constexpr int OP = 17;        // output staging pitch
 
 // Sources and destinations are slots of per-block pools: slot s of block b
@@ -131,14 +141,23 @@ struct FusedArgs {
   int* err;
 };
 
+template <bool SMALL>
 struct FusedSmem {
   int8_t B[NCOL * KW];
   int8_t A[MAXK][LT * KW];
-  double F[2][LT * FW];
+  double F[2][LT * 33];
   double O[3][LT * OP];
   double K[2][LT * NO];   // KO sums of the earlier axes, prefetched with the window (ko_add passes)
   long long base[2][LT];  // first element of each line of the tile in F[buf]
 };
+template <>
+struct FusedSmem<true> {  // output staging lives in F[buf] once the digits are made
+  int8_t B[NCOL * KW];
+  int8_t A[MAXK][LT * KW];
+  double F[2][LT * 35];
+  long long base[2][LT];
+};
+static_assert(2 * LT * OP <= LT * 35, "two staging groups fit in a window buffer");
 
 // Exact conversions between float64 and integers below 2^51 on the float64
 // and integer pipes: adding 1.5 * 2^52 puts rint(v) in the low mantissa bits
@@ -152,6 +171,19 @@ __device__ __forceinline__ double ll_to_double(long long n) {  // |n| < 2^51
   return __dsub_rn(__longlong_as_double(n + MAGIC_BITS), MAGIC);
 }
 
+// 32 lanes x N columns of 32-bit TMEM words (N = 4 or 8) into v.
+template <int N>
+__device__ __forceinline__ void tmem_ld(uint32_t addr, uint32_t (&v)[N]) {
+  if constexpr (N == 8)
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(addr));
+  else
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                 : "r"(addr));
+}
+
 __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
@@ -159,13 +191,28 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 // D2: the pass also gives the diagonal second derivative (C2 as a high and a
 // low INT8 digit); KOG: it also gives the KO term. The MMA's N holds only the
 // stencil groups the pass needs: C1 [| C2 hi | C2 lo] [| KO], 16 columns each.
-template <int R, int AXIS, bool D2, bool KOG>
-__global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
+template <int R, int AXIS, bool D2, bool KOG, bool SMALL>
+__global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel(const FusedArgs a) {
+  constexpr int FT = Cfg<SMALL>::FT, PPT = Cfg<SMALL>::PPT, OPW = Cfg<SMALL>::OPW, FW = Cfg<SMALL>::FW;
+  static_assert(!SMALL || !D2, "passes with second derivatives take the large shape");
   constexpr int NG = 1 + (D2 ? 2 : 0) + (KOG ? 1 : 0);
   constexpr int NC = NO * NG;       // MMA N and TMEM columns per digit plane
   constexpr int GKO = D2 ? 3 : 1;   // column group of KO
   extern __shared__ __align__(128) unsigned char fsm_raw[];
-  FusedSmem& sm = *reinterpret_cast<FusedSmem*>(fsm_raw);
+  FusedSmem<SMALL>& sm = *reinterpret_cast<FusedSmem<SMALL>*>(fsm_raw);
+  // TMEM columns: k planes of NC columns (a power of two of at least 32)
+  constexpr uint32_t TCOLS = SMALL ? (NC * MAXK <= 128 ? 128u : 256u) : 512u;
+  static_assert(NC * MAXK <= (int)TCOLS, "digit planes exceed the allocated TMEM columns");
+  constexpr int GKO_OUT = SMALL ? 1 : 2;  // staging group of the KO outputs
+  // output staging group g of the tile in buffer b (SMALL: inside F[b], spent by then)
+  auto obuf = [&](int b, int g) -> double* {
+    if constexpr (SMALL) return &sm.F[b][g * LT * OP];
+    else return &sm.O[g][0];
+  };
+  auto kbuf = [&](int b) -> double* {
+    if constexpr (SMALL) return nullptr;
+    else return &sm.K[b][0];
+  };
   __shared__ __align__(8) uint64_t mbar;
   __shared__ uint32_t tmem_base;
   const int tid = threadIdx.x, warp = tid >> 5;
@@ -202,7 +249,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   }
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(&tmem_base)),
-                 "r"(512));
+                 "r"(TCOLS));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -300,7 +347,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       q = q < 0 ? 0 : (q > ti.s_axis - 1 ? ti.s_axis - 1 : q);  // edge padding (derivatives.py:83-84)
       cp_async8(&sm.F[buf][r * FW + pos], src + sm.base[buf][r] + (long long)q * ti.stride);
     }
-    if (KOG && a.ko_add) {
+    if (KOG && !SMALL && a.ko_add) {
       // the KO sum this pass adds to, in the store loop's order
       const double* kos = a.dst + ti.pbase * a.dst_slots + (long long)a.ko_slot * ti.n;
       for (int i = tid; i < LT * NO; i += FT) {
@@ -309,7 +356,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
         const long long l = ti.lb * LT + rr;
         const int z = ti.z0 + o;
         if (l < ti.nlines && z < ti.len)
-          cp_async8(&sm.K[buf][i], kos + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride);
+          cp_async8(&kbuf(buf)[i], kos + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride);
       }
     }
     asm volatile("cp.async.commit_group;\n" ::: "memory");
@@ -386,14 +433,16 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       for (int s2 = 0; s2 < a.k; ++s2, dst += LT * KW) {  // plane by plane, most significant first
         const int sh = 7 * (a.k - 1 - s2);
         const uint32_t mask = s2 == 0 ? 255u : 127u;
-        uint32_t w0 = 0u, w1 = 0u;
+        uint32_t w[PPT / 4];
+#pragma unroll
+        for (int c = 0; c < PPT / 4; ++c) w[c] = 0u;
 #pragma unroll
         for (int j = 0; j < PPT; ++j) {
           const uint32_t d = (uint32_t)(X[j] >> sh) & mask;
-          if (j < 4) w0 |= d << (8 * j);
-          else w1 |= d << (8 * (j - 4));
+          w[j >> 2] |= d << (8 * (j & 3));
         }
-        *reinterpret_cast<uint2*>(dst) = make_uint2(w0, w1);
+        if constexpr (PPT == 16) *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+        else *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[1]);
       }
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
@@ -450,9 +499,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
 #pragma unroll
         for (int g = 0; g < NG; ++g) {
           const uint32_t addr = tmem + lane + (uint32_t)(NC * (s2 - 1 + h) + NO * g + oc);
-          asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
-                       : "=r"(v[h][g][0]), "=r"(v[h][g][1]), "=r"(v[h][g][2]), "=r"(v[h][g][3])
-                       : "r"(addr));
+          tmem_ld<OPW>(addr, v[h][g]);
         }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
@@ -471,9 +518,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
 #pragma unroll
       for (int g = 0; g < NG; ++g) {
         const uint32_t addr = tmem + lane + (uint32_t)(NO * g + oc);
-        asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
-                     : "=r"(v[g][0]), "=r"(v[g][1]), "=r"(v[g][2]), "=r"(v[g][3])
-                     : "r"(addr));
+        tmem_ld<OPW>(addr, v[g]);
       }
       asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
@@ -487,9 +532,9 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
     // the recombining thread's line is r too (TMEM lane = line): its exponent is sc
 #pragma unroll
     for (int o = 0; o < OPW; ++o) {
-      sm.O[0][r * OP + oc + o] = (r1[o] * sc) * w1;
-      if (D2) sm.O[1][r * OP + oc + o] = (r2[o] * sc) * w2;
-      if (KOG) sm.O[2][r * OP + oc + o] = (rk[o] * sc) * wko;
+      obuf(buf, 0)[r * OP + oc + o] = (r1[o] * sc) * w1;
+      if (D2) obuf(buf, 1)[r * OP + oc + o] = (r2[o] * sc) * w2;
+      if (KOG) obuf(buf, GKO_OUT)[r * OP + oc + o] = (rk[o] * sc) * wko;
     }
     __syncthreads();
     // ---- coalesced stores of the tile's outputs ----
@@ -500,9 +545,13 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
       const int z = ti.z0 + o;
       if (l < ti.nlines && z < ti.len && !failed) {
         double* out = a.dst + ti.pbase * a.dst_slots + sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride;
-        out[(long long)a.d1_slot * ti.n] = sm.O[0][rr * OP + o];
-        if (D2) out[(long long)a.d2_slot * ti.n] = sm.O[1][rr * OP + o];
-        if (KOG) out[(long long)a.ko_slot * ti.n] = a.ko_add ? sm.K[buf][i] + sm.O[2][rr * OP + o] : sm.O[2][rr * OP + o];
+        out[(long long)a.d1_slot * ti.n] = obuf(buf, 0)[rr * OP + o];
+        if (D2) out[(long long)a.d2_slot * ti.n] = obuf(buf, 1)[rr * OP + o];
+        if (KOG) {
+          double* kp = out + (long long)a.ko_slot * ti.n;
+          const double kv = obuf(buf, GKO_OUT)[rr * OP + o];
+          *kp = a.ko_add ? (SMALL ? *kp : kbuf(buf)[i]) + kv : kv;
+        }
       }
     }
     // the next tile's window (this thread's copies) has landed; the barrier
@@ -513,7 +562,7 @@ __global__ void __launch_bounds__(FT, 1) fused_kernel(const FusedArgs a) {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(512));
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(TCOLS));
 }
 
 }  // namespace ozaki
@@ -523,28 +572,38 @@ namespace {
 thread_local std::string g_oz_err;
 
 template <int R, int AXIS, bool D2, bool KOG>
-cudaError_t launch_fused(const ozaki::FusedArgs& m, int grid, cudaStream_t st, int dev) {
+cudaError_t launch_fused(const ozaki::FusedArgs& m, long long ntiles, int sms, cudaStream_t st, int dev) {
+  constexpr bool SMALL = !D2;
+  using C = ozaki::Cfg<SMALL>;
   static bool attr_done[64] = {false};
-  constexpr int kSmem = (int)sizeof(ozaki::FusedSmem);
+  constexpr int kSmem = (int)sizeof(ozaki::FusedSmem<SMALL>);
   if (!attr_done[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS, D2, KOG>,
+    cudaError_t e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS, D2, KOG, SMALL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(ozaki::fused_kernel<R, AXIS, D2, KOG, SMALL>,
+                               cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
     if (e != cudaSuccess) return e;
     attr_done[dev] = true;
   }
-  ozaki::fused_kernel<R, AXIS, D2, KOG><<<grid, ozaki::FT, kSmem, st>>>(m);
+  // persistent: C::CTAS CTAs per SM (the TMEM columns of a CTA allow that many)
+  const long long cap = (long long)C::CTAS * sms;
+  const int grid = (int)(ntiles < cap ? ntiles : cap);
+  ozaki::fused_kernel<R, AXIS, D2, KOG, SMALL><<<grid, C::FT, kSmem, st>>>(m);
   return cudaSuccess;
 }
 
 // The instantiation for a pass: the KO reach only matters when KO is formed.
 template <int AXIS>
-cudaError_t launch_axis(const ozaki::FusedArgs& m, int grid, cudaStream_t st, int dev, int R, bool d2, bool ko) {
+cudaError_t launch_axis(const ozaki::FusedArgs& m, int sms, cudaStream_t st, int dev, int R, bool d2, bool ko) {
+  const long long t = m.ntiles;
   if (ko) {
-    if (R == 4) return d2 ? launch_fused<4, AXIS, true, true>(m, grid, st, dev) : launch_fused<4, AXIS, false, true>(m, grid, st, dev);
-    return d2 ? launch_fused<3, AXIS, true, true>(m, grid, st, dev) : launch_fused<3, AXIS, false, true>(m, grid, st, dev);
+    if (R == 4) return d2 ? launch_fused<4, AXIS, true, true>(m, t, sms, st, dev) : launch_fused<4, AXIS, false, true>(m, t, sms, st, dev);
+    return d2 ? launch_fused<3, AXIS, true, true>(m, t, sms, st, dev) : launch_fused<3, AXIS, false, true>(m, t, sms, st, dev);
   }
-  return d2 ? launch_fused<3, AXIS, true, false>(m, grid, st, dev) : launch_fused<3, AXIS, false, false>(m, grid, st, dev);
+  return d2 ? launch_fused<3, AXIS, true, false>(m, t, sms, st, dev) : launch_fused<3, AXIS, false, false>(m, t, sms, st, dev);
 }
+
 int oz_fail(int code, const std::string& m) {
   g_oz_err = m;
   return code;
@@ -585,12 +644,11 @@ int run_bundle(cudaStream_t st, const double* F, const double* S, double* D, int
     m.ntiles = ntiles[kind];
     m.err = err;
     if (m.ntiles < 1) return 0;
-    const int grid = (int)(m.ntiles < sms ? m.ntiles : sms);  // one CTA per SM: it owns all 512 TMEM columns
     const int axis = pk.axis;
     const bool has2 = d2 >= 0, hasko = ko >= 0;
-    cudaError_t le = axis == 0 ? launch_axis<0>(m, grid, st, dev, R, has2, hasko)
-                   : (axis == 1 ? launch_axis<1>(m, grid, st, dev, R, has2, hasko)
-                                : launch_axis<2>(m, grid, st, dev, R, has2, hasko));
+    cudaError_t le = axis == 0 ? launch_axis<0>(m, sms, st, dev, R, has2, hasko)
+                   : (axis == 1 ? launch_axis<1>(m, sms, st, dev, R, has2, hasko)
+                                : launch_axis<2>(m, sms, st, dev, R, has2, hasko));
     if (le == cudaSuccess) le = cudaGetLastError();
     if (le != cudaSuccess) return oz_fail(BSSN_B200_ECUDA, std::string("ozaki launch: ") + cudaGetErrorString(le));
     return 0;
