@@ -381,7 +381,7 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
     const double wko = (1.0 / (R == 4 ? 256.0 : 64.0)) * (a.ko_sigma / ti.h);
     // (this tile's window has landed: the barrier that ended the previous
     // tile, or the prologue's, followed every thread's wait for its copies)
-    // ---- exponent and digits: the four threads of line r take 8 positions each ----
+    // ---- exponent and digits: the QT threads of line r take PPT positions each ----
     const int r = tid & (LT - 1), q4 = tid >> 7;
     const double* Fr = &sm.F[buf][r * FW + PPT * q4];
     double m = 0.0;
