@@ -158,6 +158,7 @@ struct FusedSmem<true> {  // output staging lives in F[buf] once the digits are 
   long long base[2][LT];
 };
 static_assert(2 * LT * OP <= LT * 35, "two staging groups fit in a window buffer");
+static_assert(LT * OP * 8 <= MAXK * LT * KW, "a staging group fits in the digit planes");
 
 // Exact conversions between float64 and integers below 2^51 on the float64
 // and integer pipes: adding 1.5 * 2^52 puts rint(v) in the low mantissa bits
@@ -194,7 +195,6 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src) {
 template <int R, int AXIS, bool D2, bool KOG, bool SMALL>
 __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel(const FusedArgs a) {
   constexpr int FT = Cfg<SMALL>::FT, PPT = Cfg<SMALL>::PPT, OPW = Cfg<SMALL>::OPW, FW = Cfg<SMALL>::FW;
-  static_assert(!SMALL || !D2, "passes with second derivatives take the large shape");
   constexpr int NG = 1 + (D2 ? 2 : 0) + (KOG ? 1 : 0);
   constexpr int NC = NO * NG;       // MMA N and TMEM columns per digit plane
   constexpr int GKO = D2 ? 3 : 1;   // column group of KO
@@ -202,11 +202,15 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
   FusedSmem<SMALL>& sm = *reinterpret_cast<FusedSmem<SMALL>*>(fsm_raw);
   // TMEM columns: k planes of NC columns (a power of two of at least 32)
   constexpr uint32_t TCOLS = SMALL ? (NC * MAXK <= 128 ? 128u : 256u) : 512u;
-  static_assert(NC * MAXK <= (int)TCOLS, "digit planes exceed the allocated TMEM columns");
-  constexpr int GKO_OUT = SMALL ? 1 : 2;  // staging group of the KO outputs
-  // output staging group g of the tile in buffer b (SMALL: inside F[b], spent by then)
+  // digit planes per contraction round: all of them when they fit the
+  // columns, else an even count (rounds then hold whole recombination pairs)
+  constexpr int PR = NC * MAXK <= (int)TCOLS ? MAXK : (((int)TCOLS / NC) & ~1);
+  static_assert(PR >= 2 && PR * NC <= (int)TCOLS, "a contraction round exceeds the allocated TMEM columns");
+  constexpr int GKO_OUT = (SMALL && !D2) ? 1 : 2;  // staging group of the KO outputs
+  // output staging group g of the tile in buffer b. SMALL: d1 and d2 inside
+  // F[b] and KO inside the digit planes, both spent by then.
   auto obuf = [&](int b, int g) -> double* {
-    if constexpr (SMALL) return &sm.F[b][g * LT * OP];
+    if constexpr (SMALL) return g < 2 ? &sm.F[b][g * LT * OP] : reinterpret_cast<double*>(&sm.A[0][0]);
     else return &sm.O[g][0];
   };
   auto kbuf = [&](int b) -> double* {
@@ -447,43 +451,14 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
-    // ---- thread 0 issues the contractions; while they run, the first four warps
-    // look the next tile up (its base table and sti slot were last read last
-    // tile); the barrier after the wait publishes it and everyone prefetches
-    // the next tile's window behind the recombination and stores ----
-    if (tid == 0) {
-      const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
-      for (int s2 = 0; s2 < a.k; ++s2) {
-        const uint64_t da = smem_desc(smem_u32(&sm.A[s2][0]), LT * 16, 128);
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
-            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NC * s2)),
-            "l"(da), "l"(db), "r"(idesc(NC)), "r"(0u));
-      }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                       smem_u32(&mbar))
-                   : "memory");
-    }
-    const bool more = tile + gridDim.x < ntiles;
-    if (more) lookup(tile + gridDim.x, buf ^ 1);
-    uint32_t done = 0;
-    for (long long it = 0; it < WAIT_LIMIT && !done; ++it) {
-      asm volatile(
-          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
-          : "=r"(done)
-          : "r"(smem_u32(&mbar)), "r"(phase)
-          : "memory");
-    }
-    if (__syncthreads_or(!done)) {
-      if (tid == 0) atomicExch(a.err, 1);
-      failed = true;
-    }
-    phase ^= 1u;
-    if (more && !failed) issue_window(buf ^ 1);
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // ---- recombine: warp w reads TMEM lanes 32 (w % 4).., outputs OPW (w / 4).. ----
-    const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;
-    const int oc = OPW * (warp >> 2);
+    // ---- contractions in rounds of PR digit planes, smallest planes first
+    // (one round unless the planes exceed the CTA's TMEM columns). Thread 0
+    // issues a round; during the first, the first four warps look the next
+    // tile up (its base table and sti slot were last read last tile); the
+    // barrier after the first wait publishes it and everyone prefetches the
+    // next tile's window behind the recombination and stores ----
+    const uint32_t lane = (uint32_t)((warp & 3) * 32) << 16;  // warp w reads TMEM lanes 32 (w % 4)..
+    const int oc = OPW * (warp >> 2);                           // and outputs OPW (w / 4)..
     double r1[OPW], r2[OPW], rk[OPW];
 #pragma unroll
     for (int o = 0; o < OPW; ++o) { r1[o] = 0.0; r2[o] = 0.0; rk[o] = 0.0; }
@@ -491,41 +466,109 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
     // int32 (|C2 pair| < 2^25), converted once and added with the weight of
     // plane s; an odd top plane goes alone
     double w = ldexp(1.0, -7 * a.k);  // weight of the smallest digit plane
-    int s2 = a.k - 1;
-    for (; s2 >= 1; s2 -= 2, w *= 16384.0) {
-      uint32_t v[2][NG][OPW];  // [0]: plane s2 - 1 (weight 128 w), [1]: plane s2
-#pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int g = 0; g < NG; ++g) {
-          const uint32_t addr = tmem + lane + (uint32_t)(NC * (s2 - 1 + h) + NO * g + oc);
-          tmem_ld<OPW>(addr, v[h][g]);
+    int s2 = a.k - 1;                  // planes s2 .. 0 remain
+    const bool more = tile + gridDim.x < ntiles;
+    for (int round = 0; s2 >= 0 && !failed; ++round) {
+      const int lo = s2 - PR + 1 > 0 ? s2 - PR + 1 : 0;  // this round: planes lo .. s2 at columns NC (p - lo)
+      if (tid == 0) {
+        const uint64_t db = smem_desc(smem_u32(sm.B), NC * 16, 128);
+        for (int p = lo; p <= s2; ++p) {
+          const uint64_t da = smem_desc(smem_u32(&sm.A[p][0]), LT * 16, 128);
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+              "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem + (uint32_t)(NC * (p - lo))),
+              "l"(da), "l"(db), "r"(idesc(NC)), "r"(0u));
         }
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                         smem_u32(&mbar))
+                     : "memory");
+      }
+      if (round == 0 && more) lookup(tile + gridDim.x, buf ^ 1);
+      uint32_t done = 0;
+      for (long long it = 0; it < WAIT_LIMIT && !done; ++it) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(&mbar)), "r"(phase)
+            : "memory");
+      }
+      if (__syncthreads_or(!done)) {
+        if (tid == 0) atomicExch(a.err, 1);
+        failed = true;
+      }
+      phase ^= 1u;
+      if (failed) break;
+      if (round == 0 && more) issue_window(buf ^ 1);
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      for (; s2 - 1 >= lo; s2 -= 2, w *= 16384.0) {
+        const uint32_t ca = (uint32_t)(NC * (s2 - 1 - lo)), cb = (uint32_t)(NC * (s2 - lo));
+        if constexpr (SMALL && D2) {  // one stencil at a time (registers)
+          {
+            uint32_t va[OPW], vb[OPW];
+            tmem_ld<OPW>(tmem + lane + ca + (uint32_t)oc, va);
+            tmem_ld<OPW>(tmem + lane + cb + (uint32_t)oc, vb);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
 #pragma unroll
-      for (int o = 0; o < OPW; ++o) {
-        r1[o] += ll_to_double((int)v[0][0][o] * 128 + (int)v[1][0][o]) * w;
-        if (D2) {
-          const int c2a = (int)v[0][D2 ? 1 : 0][o] * 128 + (int)v[0][D2 ? 2 : 0][o];
-          const int c2b = (int)v[1][D2 ? 1 : 0][o] * 128 + (int)v[1][D2 ? 2 : 0][o];
-          r2[o] += ll_to_double(c2a * 128 + c2b) * w;
+            for (int o = 0; o < OPW; ++o) r1[o] += ll_to_double((int)va[o] * 128 + (int)vb[o]) * w;
+          }
+          {
+            uint32_t ha[OPW], hb[OPW], la[OPW], lb2[OPW];  // C2 high and low digits of planes s2 - 1, s2
+            tmem_ld<OPW>(tmem + lane + ca + (uint32_t)(NO + oc), ha);
+            tmem_ld<OPW>(tmem + lane + cb + (uint32_t)(NO + oc), hb);
+            tmem_ld<OPW>(tmem + lane + ca + (uint32_t)(2 * NO + oc), la);
+            tmem_ld<OPW>(tmem + lane + cb + (uint32_t)(2 * NO + oc), lb2);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int o = 0; o < OPW; ++o) {
+              const int c2a = (int)ha[o] * 128 + (int)la[o];
+              const int c2b = (int)hb[o] * 128 + (int)lb2[o];
+              r2[o] += ll_to_double(c2a * 128 + c2b) * w;
+            }
+          }
+          if (KOG) {
+            uint32_t va[OPW], vb[OPW];
+            tmem_ld<OPW>(tmem + lane + ca + (uint32_t)(NO * GKO + oc), va);
+            tmem_ld<OPW>(tmem + lane + cb + (uint32_t)(NO * GKO + oc), vb);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int o = 0; o < OPW; ++o) rk[o] += ll_to_double((int)va[o] * 128 + (int)vb[o]) * w;
+          }
+        } else {
+          uint32_t v[2][NG][OPW];  // [0]: plane s2 - 1 (weight 128 w), [1]: plane s2
+#pragma unroll
+          for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int g = 0; g < NG; ++g) tmem_ld<OPW>(tmem + lane + (h ? cb : ca) + (uint32_t)(NO * g + oc), v[h][g]);
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+          for (int o = 0; o < OPW; ++o) {
+            r1[o] += ll_to_double((int)v[0][0][o] * 128 + (int)v[1][0][o]) * w;
+            if (D2) {
+              const int c2a = (int)v[0][D2 ? 1 : 0][o] * 128 + (int)v[0][D2 ? 2 : 0][o];
+              const int c2b = (int)v[1][D2 ? 1 : 0][o] * 128 + (int)v[1][D2 ? 2 : 0][o];
+              r2[o] += ll_to_double(c2a * 128 + c2b) * w;
+            }
+            if (KOG) rk[o] += ll_to_double((int)v[0][KOG ? GKO : 0][o] * 128 + (int)v[1][KOG ? GKO : 0][o]) * w;
+          }
         }
-        if (KOG) rk[o] += ll_to_double((int)v[0][KOG ? GKO : 0][o] * 128 + (int)v[1][KOG ? GKO : 0][o]) * w;
       }
-    }
-    if (s2 == 0) {
-      uint32_t v[NG][OPW];
+      if (s2 == lo) {  // lo == 0: the odd top plane alone
+        uint32_t v[NG][OPW];
 #pragma unroll
-      for (int g = 0; g < NG; ++g) {
-        const uint32_t addr = tmem + lane + (uint32_t)(NO * g + oc);
-        tmem_ld<OPW>(addr, v[g]);
+        for (int g = 0; g < NG; ++g) tmem_ld<OPW>(tmem + lane + (uint32_t)(NC * (s2 - lo) + NO * g + oc), v[g]);
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+        for (int o = 0; o < OPW; ++o) {
+          r1[o] += (double)(int)v[0][o] * w;
+          if (D2) r2[o] += (double)((int)v[D2 ? 1 : 0][o] * 128 + (int)v[D2 ? 2 : 0][o]) * w;
+          if (KOG) rk[o] += (double)(int)v[KOG ? GKO : 0][o] * w;
+        }
+        s2 = -1;
       }
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-      for (int o = 0; o < OPW; ++o) {
-        r1[o] += (double)(int)v[0][o] * w;
-        if (D2) r2[o] += (double)((int)v[D2 ? 1 : 0][o] * 128 + (int)v[D2 ? 2 : 0][o]) * w;
-        if (KOG) rk[o] += (double)(int)v[KOG ? GKO : 0][o] * w;
+      if (s2 >= 0) {  // every warp has read this round's columns before the next round's contractions
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       }
     }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
@@ -573,7 +616,7 @@ thread_local std::string g_oz_err;
 
 template <int R, int AXIS, bool D2, bool KOG>
 cudaError_t launch_fused(const ozaki::FusedArgs& m, long long ntiles, int sms, cudaStream_t st, int dev) {
-  constexpr bool SMALL = !D2;
+  constexpr bool SMALL = true;
   using C = ozaki::Cfg<SMALL>;
   static bool attr_done[64] = {false};
   constexpr int kSmem = (int)sizeof(ozaki::FusedSmem<SMALL>);
