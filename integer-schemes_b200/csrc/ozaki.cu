@@ -101,12 +101,15 @@ inline long long pass_tiles(const bssn_b200_block& b, const PassKind& k) {
 // the outputs go out through shared memory so that the stores are coalesced
 // as well. The next tile's window is prefetched while a tile is contracted.
 //
-// Two shapes: passes with second derivatives (N = 48 or 64: all 512 TMEM
-// columns for k = 6..8) run one 512-thread CTA per SM; the others (N = 16 or
-// 32: at most 256 columns) run two 256-thread CTAs per SM in ~106 KB of
-// shared memory each (output staging inside the spent window buffer, KO sums
-// read back from global memory), so that one CTA's barriers overlap the
-// other's work.
+// Two shapes. The small one (the one launched) runs two 256-thread CTAs per
+// SM in ~106 KB of shared memory each: at most 256 TMEM columns, the digit
+// planes contracted in rounds that fit them (one round for N = 16 or 32,
+// two for the passes with second derivatives), output staging inside the
+// spent window buffer and digit planes, the KO sums a pass adds to loaded
+// into registers during the contractions; one CTA's barriers then overlap
+// the other's work. The large one (one 512-thread CTA per SM, all 512
+// columns, one round, KO sums prefetched into shared memory) measured
+// slower and is kept as the reference shape of the same tile loop.
 template <bool SMALL>
 struct Cfg {
   static constexpr int FT = SMALL ? 256 : 512;  // threads
@@ -451,6 +454,25 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     __syncthreads();
+    // the KO sums this pass adds to (SMALL has no shared-memory room for them):
+    // loaded into registers now, in the store loop's order, so that they
+    // arrive during the contractions
+    constexpr int SPT = LT * NO / FT;  // outputs per thread in the store loop
+    double kpre[SPT];
+    if constexpr (SMALL && KOG) {
+      if (a.ko_add) {
+        const double* kos = a.dst + ti.pbase * a.dst_slots + (long long)a.ko_slot * ti.n;
+#pragma unroll
+        for (int j = 0; j < SPT; ++j) {
+          const int i = tid + j * FT;
+          const int rr = zaxis ? i / NO : i % LT;
+          const int o = zaxis ? i % NO : i / LT;
+          const int z = ti.z0 + o;
+          kpre[j] = (ti.lb * LT + rr < ti.nlines && z < ti.len)
+                        ? kos[sm.base[buf][rr] + (long long)(ti.m_axis + z) * ti.stride] : 0.0;
+        }
+      }
+    }
     // ---- contractions in rounds of PR digit planes, smallest planes first
     // (one round unless the planes exceed the CTA's TMEM columns). Thread 0
     // issues a round; during the first, the first four warps look the next
@@ -581,7 +603,9 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
     }
     __syncthreads();
     // ---- coalesced stores of the tile's outputs ----
-    for (int i = tid; i < LT * NO; i += FT) {
+#pragma unroll
+    for (int j = 0; j < SPT; ++j) {
+      const int i = tid + j * FT;
       const int rr = zaxis ? i / NO : i % LT;
       const int o = zaxis ? i % NO : i / LT;
       const long long l = ti.lb * LT + rr;
@@ -593,7 +617,7 @@ __global__ void __launch_bounds__(Cfg<SMALL>::FT, Cfg<SMALL>::CTAS) fused_kernel
         if (KOG) {
           double* kp = out + (long long)a.ko_slot * ti.n;
           const double kv = obuf(buf, GKO_OUT)[rr * OP + o];
-          *kp = a.ko_add ? (SMALL ? *kp : kbuf(buf)[i]) + kv : kv;
+          *kp = a.ko_add ? (SMALL ? kpre[j] : kbuf(buf)[i]) + kv : kv;
         }
       }
     }
