@@ -43,9 +43,11 @@ UNIT = "Mpoint-updates/s"
 FLOPS_PER_POINT = 6714      # algorithmic FP64 flops per RHS point-update (oracle/count_flops.py): algebra 4,278 + derivatives 2,436
 KO_FLOPS_PER_POINT = 936    # 24 fields x 3 axes x (7 taps: 7 mul + 6 add)
 STAGE_BYTES = 960           # read Y, U, ACC; write ACC, Y_next (5 x 24 x 8 B)
-# DRAM bytes per point of one stage launch, dram__bytes_read.sum + dram__bytes_write.sum
-# from an ncu capture of the 102^3 case (stage 1), scaled to a launch by its points
-TRAFFIC_BYTES_PER_POINT = 962
+# DRAM bytes per evaluated point of one stage launch, dram__bytes_read.sum +
+# dram__bytes_write.sum from an ncu capture of the stage-1 kernel on the 102^3
+# case, scaled to a launch by its points (the capture is named here)
+TRAFFIC_BYTES_PER_POINT = 988
+TRAFFIC_SOURCE = "ncu capture, profiles/stream_kernel_stage_102.md (988 B per evaluated point)"
 LAST_STAGE_BYTES = 768      # read Y, U, ACC; write U_new
 
 
@@ -76,6 +78,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-fp64-peak", action="store_true")
     ap.add_argument("--no-stage-timing", action="store_true")
+    ap.add_argument("--no-ozaki", action="store_true",
+                    help="bl128: skip the Ozaki INT8 RHS measured beside the float64 one")
     return ap.parse_args()
 
 
@@ -386,24 +390,32 @@ def bench_b200(args):
                        "neighbouring steps' compute"}
         del pipe
 
+    # the Ozaki INT8 half of the metric, on the same state (outside the timed region)
+    ozaki = None
+    if not args.no_ozaki and not msrk:
+        ozaki = ozaki_leg(torch, dev, U0, grid, dt, args.ozaki_k or 6, max(args.warmup, 3))
+
     peaks, peak_kind = measured_peaks()
     fp64_peak = measure_fp64_peak(torch, dev) if (rank == 0 and not args.no_fp64_peak) else None
 
     value = interior * 4 * args.steps * world / (ms * 1e-3) / 1e6
     mean_stage = statistics.mean(stage_ms[:3]) if stage_ms else ms / args.steps / nstage
-    achieved_gbs = npts * STAGE_BYTES / (mean_stage * 1e-3) / 1e9
-    flops = npts * (FLOPS_PER_POINT + KO_FLOPS_PER_POINT)
+    # algorithmic bytes and flops of the interior point-updates a launch delivers
+    # (the unit the metric credits); the kernel also evaluates the ghost points
+    achieved_gbs = interior * STAGE_BYTES / (mean_stage * 1e-3) / 1e9
+    flops = interior * (FLOPS_PER_POINT + KO_FLOPS_PER_POINT)
     achieved_tf = flops / (mean_stage * 1e-3) / 1e12
     roofline = {"bound": "hbm", "achieved": achieved_gbs, "peak": peaks.get("hbm_gbs"),
                 "unit": "GB/s", "frac": achieved_gbs / peaks.get("hbm_gbs"),
                 "traffic": TRAFFIC_BYTES_PER_POINT * npts, "peak_source": f"{peak_kind} hbm_gbs",
+                "traffic_source": TRAFFIC_SOURCE,
                 "kernel": "bssn::stream_kernel<3, MODE_STAGE, Shape<4,4,16>> (stages 0-2)",
-                "bytes_per_point": STAGE_BYTES, "points_per_launch": npts,
-                "launch_ms": mean_stage}
+                "bytes_per_point_update": STAGE_BYTES, "point_updates_per_launch": interior,
+                "points_evaluated_per_launch": npts, "launch_ms": mean_stage}
     roofline_fp64 = {"bound": "fp64", "achieved": achieved_tf, "peak": fp64_peak,
                      "unit": "TFLOP/s", "frac": (achieved_tf / fp64_peak) if fp64_peak else None,
                      "peak_source": "cuBLAS DGEMM 8192^3 measured in this run",
-                     "flops_per_point": FLOPS_PER_POINT + KO_FLOPS_PER_POINT}
+                     "flops_per_point_update": FLOPS_PER_POINT + KO_FLOPS_PER_POINT}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -434,7 +446,7 @@ def bench_b200(args):
                    "l2": "inputs larger than L2 (462 MB state)", "parallelism": f"replicas x{world}"},
         "clocks": clk, "gpu_launches": (nstage + 1) * args.steps, "finite": finite,
         "stage_ms": stage_ms, "roofline": roofline, "roofline_fp64": roofline_fp64,
-        "e2e": e2e, "cpu_baseline": cpu,
+        "e2e": e2e, "cpu_baseline": cpu, "ozaki": ozaki,
     }
     if tracked is not None:
         line["constraints"] = tracked
@@ -444,6 +456,58 @@ def bench_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def ozaki_leg(torch, dev, U, grid, dt, k: int, reps: int):
+    """The RHS of the bench state through the Ozaki INT8 derivative path (k
+    digit planes, tcgen05 kind::i8, float64 algebra) beside the fused float64
+    RHS of the same state: time per RHS (CUDA events, median of 5 batches),
+    Mpoint-updates/s of interior points, each field's max|oz - fp64| /
+    max|fp64|, and bit-identity over 5 runs."""
+    from bssn3d_b200.fused_rhs import device_scalars, pack_S, rhs_tensor
+    from bssn3d_b200.ozaki import OzakiDerivatives
+    S = device_scalars(pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0),
+                              grid.dy, grid.dz), dev)
+    stream = torch.cuda.current_stream(dev)
+    interior = grid.interior_points
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize(dev)
+        meds = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                fn()
+            b.record(stream)
+            b.synchronize()
+            meds.append(a.elapsed_time(b) / reps)
+        return statistics.median(meds)
+
+    ref = rhs_tensor(U, S)
+    out_fp = torch.empty_like(ref)
+    fp_ms = timed(lambda: rhs_tensor(U, S, out_fp))
+    oz = OzakiDerivatives(U.shape[1:], k, device=dev)
+    oz_ms = timed(lambda: oz.rhs(U, S))
+    got = oz.rhs(U, S)
+    same = all(torch.equal(oz.rhs(U, S), got) for _ in range(4))
+    oz.check()
+    num = (got - ref).reshape(24, -1).abs().amax(dim=1)
+    den = ref.reshape(24, -1).abs().amax(dim=1).clamp_min(1e-300)
+    err = torch.where(num == 0, torch.zeros_like(num), num / den)
+    del oz, got, ref, out_fp
+    torch.cuda.empty_cache()
+    fp_rate = interior / (fp_ms * 1e-3) / 1e6
+    oz_rate = interior / (oz_ms * 1e-3) / 1e6
+    return {"k": k, "value": oz_rate, "unit": UNIT, "ms_per_rhs": oz_ms,
+            "fp64_value": fp_rate, "fp64_ms_per_rhs": fp_ms, "ratio_to_fp64": oz_rate / fp_rate,
+            "max_field_err_vs_fp64": float(err.max()), "worst_field": int(err.argmax()),
+            "per_field_err_vs_fp64": [float(x) for x in err.cpu()],
+            "bit_identical_5_runs": same, "bar": 1e-10,
+            "what": "one RHS of the bench state: Ozaki INT8 derivatives (bssn_b200_ozaki_derivatives) + "
+                    "float64 algebra (bssn_b200_rhs_algebra) vs the fused float64 RHS (bssn_b200_rhs)"}
 
 
 def track_constraints(advance, norms, total: int, every: int):

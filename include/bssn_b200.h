@@ -181,7 +181,9 @@ int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int
  * to 256 SMs and a launch that would need more slots is rejected with
  * BSSN_B200_EINVAL. Inputs and outputs are still the caller's. The first call
  * on a device resolves the array's device address with cudaGetSymbolAddress,
- * so make that first call before any stream capture. All calls share the
+ * so make that first call before any stream capture. The address is kept per
+ * device for the life of the process: after cudaDeviceReset the library must
+ * be reloaded before this entry point is called again. All calls share the
  * array (each call overwrites the slots it reads, so nothing needs clearing):
  * calls that overlap on the GPU — on two streams, or from two host threads —
  * race. No counterpart in the reference. */

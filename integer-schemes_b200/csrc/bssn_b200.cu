@@ -22,6 +22,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
@@ -813,7 +814,10 @@ __global__ void norm_finalize_kernel(const double* __restrict__ partials, int np
 // callers that cannot allocate device memory. It is a file-scope device array:
 // every GPU that loads this library holds it (4 KB) until the process exits,
 // and every call of that entry point reuses it.
-constexpr int kStaticNormCtas = 256;  // CTAs whose partial sums fit (2 doubles each)
+// CTAs whose partial sums fit (2 doubles each). The norm launch runs at most
+// one CTA per SM, so 256 covers every GPU with up to 256 SMs (B200: 148); a
+// GPU with more is refused by the entry point's size check.
+constexpr int kStaticNormCtas = 256;
 static __device__ __align__(256) double g_static_norm_partials[2 * kStaticNormCtas];
 
 // t <- t + dt in the device scalar pack, between captured RK4 steps
@@ -1346,12 +1350,14 @@ int bssn_b200_constraint_norms_static(void* stream, const double* F, const doubl
   if (dev < 0 || dev >= kMaxDev) return fail(BSSN_B200_EINVAL, "constraint_norms_static: device ordinal out of range");
   // In host code g_static_norm_partials names a host-side stand-in, not device
   // memory: resolve its address on this device once, with the device current.
-  static double* addr[kMaxDev] = {nullptr};
-  if (!addr[dev]) {
-    double* p = nullptr;
-    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), bssn::g_static_norm_partials);
+  // Two host threads that race here resolve the same address; the atomic slot
+  // makes the publication well defined.
+  static std::atomic<double*> addr[kMaxDev];
+  double* partials = addr[dev].load(std::memory_order_acquire);
+  if (!partials) {
+    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&partials), bssn::g_static_norm_partials);
     if (e != cudaSuccess) return cuda_fail("cudaGetSymbolAddress(static norm partials)", e);
-    addr[dev] = p;
+    addr[dev].store(partials, std::memory_order_release);
   }
   bssn::Args a{};
   int grid = 0;
@@ -1362,7 +1368,7 @@ int bssn_b200_constraint_norms_static(void* stream, const double* F, const doubl
                                       " CTA partial sums but the static array holds " +
                                       std::to_string(bssn::kStaticNormCtas) +
                                       "; use bssn_b200_constraint_norms with a caller buffer");
-  return bssn_b200_constraint_norms(stream, F, S, Sx, Sy, Sz, ng, addr[dev],
+  return bssn_b200_constraint_norms(stream, F, S, Sx, Sy, Sz, ng, partials,
                                     sizeof(double) * 2 * bssn::kStaticNormCtas, OUT2);
 }
 

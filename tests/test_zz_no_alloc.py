@@ -6,9 +6,9 @@ stream capture would break the capture by allocating, and some real-time loops
 forbid allocation outright. ``bssn_b200_constraint_norms_static`` serves them:
 it keeps its per-CTA partial sums in a static device array inside the library
 instead of a caller-provided scratch buffer. This test calls it through the C
-ABI twice in a row and checks both results against the scratch-buffer entry
-point ``bssn_b200_constraint_norms``, to the 1e-12 relative tolerance of the
-other parity tests. The file is named to be collected last.
+ABI twice in a row, on two different states, and checks both results against
+the scratch-buffer entry point ``bssn_b200_constraint_norms``, to the 1e-12
+relative tolerance of the other parity tests. The file is named to be collected last.
 """
 
 import ctypes
@@ -35,19 +35,27 @@ def test_static_norms_match_scratch_norms_twice():
 
     need = int(lib.bssn_b200_norms_scratch_bytes())
     scratch = torch.empty(max(need // 8, 2), dtype=torch.float64, device=dev)
-    ref = torch.empty(2, dtype=torch.float64, device=dev)
-    _lib.check(lib.bssn_b200_constraint_norms(stream, Ud.data_ptr(), S.data_ptr(), Sx, Sy, Sz,
-                                              grid.ng, scratch.data_ptr(), scratch.numel() * 8,
-                                              ref.data_ptr()))
-    expect = ref.cpu().numpy()
-    assert np.all(np.isfinite(expect)) and expect[0] > 0
 
-    for _ in range(2):
+    def with_scratch(F):
+        ref = torch.empty(2, dtype=torch.float64, device=dev)
+        _lib.check(lib.bssn_b200_constraint_norms(stream, F.data_ptr(), S.data_ptr(), Sx, Sy, Sz,
+                                                  grid.ng, scratch.data_ptr(), scratch.numel() * 8,
+                                                  ref.data_ptr()))
+        return ref.cpu().numpy()
+
+    # the second call sees a different state, so a call that left stale
+    # partial sums of the first one in the shared array would show
+    Vd = Ud.clone()
+    Vd[12:18] += 1e-2   # a traceful A~ changes both the Hamiltonian and momentum norms
+    for F in (Ud, Vd):
+        expect = with_scratch(F)
+        assert np.all(np.isfinite(expect)) and expect[0] > 0
         out = torch.full((2,), np.nan, dtype=torch.float64, device=dev)
-        _lib.check(lib.bssn_b200_constraint_norms_static(stream, Ud.data_ptr(), S.data_ptr(),
+        _lib.check(lib.bssn_b200_constraint_norms_static(stream, F.data_ptr(), S.data_ptr(),
                                                          Sx, Sy, Sz, grid.ng, out.data_ptr()))
         got = out.cpu().numpy()
         np.testing.assert_allclose(got, expect, rtol=1e-12, atol=0)
+    assert not np.allclose(with_scratch(Ud), with_scratch(Vd), rtol=1e-6)
 
 
 def test_static_norms_reject_an_empty_interior():
