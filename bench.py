@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-stage-timing", action="store_true")
     ap.add_argument("--no-ozaki", action="store_true",
                     help="bl128: skip the Ozaki INT8 RHS measured beside the float64 one")
+    ap.add_argument("--no-m4", action="store_true",
+                    help="bl128: skip the reference's M4 CUDA RHS measured beside the fused one")
     return ap.parse_args()
 
 
@@ -390,10 +392,13 @@ def bench_b200(args):
                        "neighbouring steps' compute"}
         del pipe
 
-    # the Ozaki INT8 half of the metric, on the same state (outside the timed region)
-    ozaki = None
+    # the Ozaki INT8 half of the metric and the reference's M4 CUDA kernel, on
+    # the same state (outside the timed region)
+    ozaki = m4 = None
     if not args.no_ozaki and not msrk:
         ozaki = ozaki_leg(torch, dev, U0, grid, dt, args.ozaki_k or 6, max(args.warmup, 3))
+    if not args.no_m4 and not msrk:
+        m4 = m4_leg(torch, dev, U0, grid, dt, max(args.warmup, 3))
 
     peaks, peak_kind = measured_peaks()
     fp64_peak = measure_fp64_peak(torch, dev) if (rank == 0 and not args.no_fp64_peak) else None
@@ -446,7 +451,8 @@ def bench_b200(args):
                    "l2": "inputs larger than L2 (462 MB state)", "parallelism": f"replicas x{world}"},
         "clocks": clk, "gpu_launches": (nstage + 1) * args.steps, "finite": finite,
         "stage_ms": stage_ms, "roofline": roofline, "roofline_fp64": roofline_fp64,
-        "e2e": e2e, "cpu_baseline": cpu, "ozaki": ozaki,
+        "e2e": e2e, "cpu_baseline": cpu, "ozaki": ozaki, "m4_reference": m4,
+        "xla_reference": {"value": None, "unavailable": XLA_UNAVAILABLE},
     }
     if tracked is not None:
         line["constraints"] = tracked
@@ -458,39 +464,99 @@ def bench_b200(args):
         print(json.dumps(line), flush=True)
 
 
+M4_LIB = ROOT / "baseline" / "_ref" / "m4" / "libm4_rhs.so"
+XLA_UNAVAILABLE = ("unavailable on this box: the reference's XLA-verbatim path needs jax 0.9.2, which is "
+                   "not installed on the B200 machine (import jax -> ModuleNotFoundError) and cannot be "
+                   "installed offline")
+
+
+def _timed_rhs(torch, dev, fn, reps: int) -> float:
+    """ms per call: 3 warm-up calls, then the median of 5 batches of ``reps``
+    calls, CUDA events on the current stream."""
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(3):
+        fn()
+    torch.cuda.synchronize(dev)
+    meds = []
+    for _ in range(5):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        meds.append(a.elapsed_time(b) / reps)
+    return statistics.median(meds)
+
+
+def _bench_S(torch, dev, grid, dt):
+    from bssn3d_b200.fused_rhs import device_scalars, pack_S
+    return device_scalars(pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0),
+                                 grid.dy, grid.dz), dev)
+
+
+def m4_leg(torch, dev, U, grid, dt, reps: int):
+    """The reference's own M4 fused CUDA RHS (3D/src/bssn3d/cuda/rhs_fused.cu,
+    generated by its gen_fused.py and compiled for sm_100a by
+    baseline/m4/build_m4.py) on the bench state, beside this project's fused
+    RHS (bssn_b200_rhs) on the same state: ms per RHS, Mpoint-updates/s of
+    interior points, and the per-field difference between the two outputs.
+    The M4 kernel is 2.28x the reference's XLA-verbatim RHS on its own H100
+    measurement (README.md:6-8), the closest GPU anchor of the reference that
+    runs here."""
+    import ctypes
+    from bssn3d_b200.fused_rhs import rhs_tensor
+    if not M4_LIB.exists():
+        return {"value": None, "unavailable": f"{M4_LIB.relative_to(ROOT)} not built "
+                                              "(python baseline/m4/build_m4.py where the reference tree is)"}
+    lib = ctypes.CDLL(str(M4_LIB))
+    lib.m4_rhs.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_int] * 4
+    lib.m4_attributes.argtypes = [ctypes.POINTER(ctypes.c_int)] * 2
+    S = _bench_S(torch, dev, grid, dt)
+    _, Sx, Sy, Sz = U.shape
+    out_m4 = torch.empty_like(U)
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def m4():
+        rc = lib.m4_rhs(stream, U.data_ptr(), S.data_ptr(), out_m4.data_ptr(), Sx, Sy, Sz, 128)
+        if rc != 0:
+            raise RuntimeError(f"M4 launch failed: cudaError {rc}")
+    out_b = torch.empty_like(U)
+    m4_ms = _timed_rhs(torch, dev, m4, reps)
+    b_ms = _timed_rhs(torch, dev, lambda: rhs_tensor(U, S, out_b), reps)
+    num = (out_m4 - out_b).reshape(24, -1).abs().amax(dim=1)
+    den = out_b.reshape(24, -1).abs().amax(dim=1).clamp_min(1e-300)
+    err = torch.where(num == 0, torch.zeros_like(num), num / den)
+    regs, local = ctypes.c_int(0), ctypes.c_int(0)
+    lib.m4_attributes(ctypes.byref(regs), ctypes.byref(local))
+    interior = grid.interior_points
+    m4_rate = interior / (m4_ms * 1e-3) / 1e6
+    b_rate = interior / (b_ms * 1e-3) / 1e6
+    del out_m4, out_b
+    torch.cuda.empty_cache()
+    return {"value": m4_rate, "unit": UNIT, "ms_per_rhs": m4_ms, "registers": regs.value,
+            "local_bytes_per_thread": local.value, "fused_value": b_rate, "fused_ms_per_rhs": b_ms,
+            "fused_over_m4": m4_ms / b_ms, "max_field_diff_vs_fused": float(err.max()),
+            "what": "one RHS of the bench state (no KO): the reference's M4 kernel "
+                    "(baseline/_ref/m4/libm4_rhs.so, 1 thread per padded point, 128-thread blocks) "
+                    "vs bssn_b200_rhs"}
+
+
 def ozaki_leg(torch, dev, U, grid, dt, k: int, reps: int):
     """The RHS of the bench state through the Ozaki INT8 derivative path (k
     digit planes, tcgen05 kind::i8, float64 algebra) beside the fused float64
     RHS of the same state: time per RHS (CUDA events, median of 5 batches),
     Mpoint-updates/s of interior points, each field's max|oz - fp64| /
     max|fp64|, and bit-identity over 5 runs."""
-    from bssn3d_b200.fused_rhs import device_scalars, pack_S, rhs_tensor
+    from bssn3d_b200.fused_rhs import rhs_tensor
     from bssn3d_b200.ozaki import OzakiDerivatives
-    S = device_scalars(pack_S(2.0, 0.06, dt, grid.dx, 0.6, 20.0, 0.0, (1, 1, 1, 1), (1, 0),
-                              grid.dy, grid.dz), dev)
-    stream = torch.cuda.current_stream(dev)
+    S = _bench_S(torch, dev, grid, dt)
     interior = grid.interior_points
-
-    def timed(fn):
-        for _ in range(3):
-            fn()
-        torch.cuda.synchronize(dev)
-        meds = []
-        for _ in range(5):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            for _ in range(reps):
-                fn()
-            b.record(stream)
-            b.synchronize()
-            meds.append(a.elapsed_time(b) / reps)
-        return statistics.median(meds)
-
     ref = rhs_tensor(U, S)
     out_fp = torch.empty_like(ref)
-    fp_ms = timed(lambda: rhs_tensor(U, S, out_fp))
+    fp_ms = _timed_rhs(torch, dev, lambda: rhs_tensor(U, S, out_fp), reps)
     oz = OzakiDerivatives(U.shape[1:], k, device=dev)
-    oz_ms = timed(lambda: oz.rhs(U, S))
+    oz_ms = _timed_rhs(torch, dev, lambda: oz.rhs(U, S), reps)
     got = oz.rhs(U, S)
     same = all(torch.equal(oz.rhs(U, S), got) for _ in range(4))
     oz.check()

@@ -10,15 +10,20 @@ sqrt and exp one each — and adds the separable derivative count and the KO6
 taps. bench.py pins the result as FLOPS_PER_POINT and KO_FLOPS_PER_POINT.
 
     python oracle/count_flops.py [path/to/bssneqs_SSL_HD_dxsq.cpp]
+
+Without an argument the file is taken from the reference root named by
+$INTEGER_SCHEMES_REFERENCE, else from the read-only mount the reference has
+in the build container.
 """
 
 from __future__ import annotations
 
+import os
 import re
 import sys
 from pathlib import Path
 
-DEFAULT = Path("/root/reference/3D/src/bssn3d/vendor/bssneqs_SSL_HD_dxsq.cpp")
+DEFAULT = Path(os.environ.get("INTEGER_SCHEMES_REFERENCE", "/root/reference")) / "3D/src/bssn3d/vendor/bssneqs_SSL_HD_dxsq.cpp"
 
 _LIT = r"\d+(?:\.\d*)?(?:[eE][-+]?\d+)?"
 _FRACTION = re.compile(rf"\(\s*{_LIT}\s*/\s*{_LIT}\s*\)")
