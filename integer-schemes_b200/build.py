@@ -20,7 +20,9 @@ PKG = HERE / "bssn3d_b200"
 LIB = PKG / "libbssn_b200.so"
 ROOT = HERE.parent
 
-SOURCES = [CSRC / "bssn_b200.cu", CSRC / "ozaki.cu", CSRC / "amr_fill.cu"]
+SOURCES = [CSRC / "bssn_b200.cu", CSRC / "stream_rhs.cu", CSRC / "stream_stage.cu", CSRC / "stream_msrk.cu",
+           CSRC / "stream_batch3.cu", CSRC / "stream_batch4.cu", CSRC / "ozaki.cu", CSRC / "amr_fill.cu"]
+OBJ_DIR = HERE / "_build"
 HEADERS = sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.h")) + [ROOT / "include" / "bssn_b200.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -48,21 +50,39 @@ def up_to_date() -> bool:
     return all(p.stat().st_mtime <= t for p in SOURCES + HEADERS + [Path(__file__)])
 
 
+def _compile(src: Path) -> tuple:
+    obj = OBJ_DIR / (src.stem + ".o")
+    cmd = [nvcc(), *ARCH, *host_compiler(), "-O3", "-lineinfo", "-std=c++17",
+           "-Xptxas", "-v", "-Xcompiler", "-fPIC", "-diag-suppress", "177",
+           "-c", str(src), "-o", str(obj)]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    return src, obj, proc
+
+
 def build(verbose: bool = False, force: bool = False) -> Path:
+    """Compile every translation unit in parallel, then link the shared library."""
     if not force and up_to_date():
         return LIB
-    cmd = [nvcc(), *ARCH, *host_compiler(), "-O3", "-lineinfo", "-std=c++17",
-           "-Xptxas", "-v", "-shared", "-Xcompiler", "-fPIC",
-           "-diag-suppress", "177",
-           "-o", str(LIB), *map(str, SOURCES)]
-    proc = subprocess.run(cmd, capture_output=True, text=True)
+    from concurrent.futures import ThreadPoolExecutor
+    OBJ_DIR.mkdir(exist_ok=True)
+    workers = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as pool:
+        results = list(pool.map(_compile, SOURCES))
+    report = []
+    for src, obj, proc in results:
+        report.append(proc.stderr)
+        if proc.returncode != 0:
+            sys.stderr.write(proc.stdout + proc.stderr)
+            raise RuntimeError(f"nvcc failed on {src.name} ({proc.returncode})")
+    link = [nvcc(), *ARCH, *host_compiler(), "-shared", "-o", str(LIB), *[str(o) for _, o, _ in results]]
+    proc = subprocess.run(link, capture_output=True, text=True)
     if proc.returncode != 0:
         sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError(f"nvcc failed ({proc.returncode})")
-    report = PKG / "ptxas_report.txt"
-    report.write_text(proc.stderr)
+        raise RuntimeError(f"link failed ({proc.returncode})")
+    text = "".join(report)
+    (PKG / "ptxas_report.txt").write_text(text)
     if verbose:
-        sys.stdout.write(proc.stderr)
+        sys.stdout.write(text)
     return LIB
 
 

@@ -7,6 +7,7 @@
 #include <string>
 
 namespace bssn_host {
+constexpr int kMaxDev = 64;  // device ordinals with per-device caches
 int fail(int code, const std::string& msg);
 int cuda_fail(const char* what, cudaError_t e);
 int device_sms(int* sms);
