@@ -17,10 +17,10 @@
 // constraints.
 //
 // Stencils follow 3D/src/bssn3d/derivative_bundle.py:31-48 and
-// common/src/mcs_common/derivatives.py:78-106: pre-scaled taps summed from
-// the lowest offset, index clamped at the array ends, mixed second
-// derivatives as a first derivative along the lower axis, then along the
-// higher axis of that result.
+// common/src/mcs_common/derivatives.py:35-106: the centred sixth-order
+// coefficients (integer sums of paired taps, scaled once), index clamped at
+// the array ends, mixed second derivatives as a first derivative along the
+// lower axis, then along the higher axis of that result.
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -47,50 +47,37 @@ template <int R>
 __device__ __forceinline__ void field_derivs(const double* __restrict__ t, int c, int f, const Weights& W,
                                              bool ko, double* __restrict__ out, long long n) {
   constexpr int st[3] = {TileGeom<R>::SX, TileGeom<R>::SY, 1};
+  double kacc = 0.0;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    double acc = 0.0;
+    double v[2 * R + 1];
 #pragma unroll
-    for (int k = 0; k < 7; ++k)
-      if (k != 3) acc = tap(acc, W.w1[a][k], t[c + (k - 3) * st[a]]);
-    out[(long long)d1slot(f, a) * n] = acc;
+    for (int k = 0; k <= 2 * R; ++k) v[k] = t[c + (k - R) * st[a]];
+    out[(long long)d1slot(f, a) * n] =
+        __dmul_rn(c1_sum(v[R - 3], v[R - 2], v[R - 1], v[R + 1], v[R + 2], v[R + 3]), W.f1[a]);
+    const double s1 = __dadd_rn(v[R + 1], v[R - 1]), s2 = __dadd_rn(v[R + 2], v[R - 2]),
+                 s3 = __dadd_rn(v[R + 3], v[R - 3]);
+    if (has_d2(f)) out[(long long)d2slot(f, sym(a, a)) * n] = __dmul_rn(c2_sum(v[R], s1, s2, s3), W.f2[a]);
+    if (ko) {
+      const double sk = R == 4 ? ko8_sum(v[R], s1, s2, s3, __dadd_rn(v[2 * R], v[0])) : ko6_sum(v[R], s1, s2, s3);
+      kacc = __dadd_rn(kacc, __dmul_rn(sk, W.fk[a]));
+    }
   }
   if (has_d2(f)) {
+    // mixed: the unscaled first-derivative sums along i at the 6 offsets along
+    // j, differentiated along j, scaled by f1_i * f1_j
+    constexpr int PI[3] = {0, 0, 1}, PJ[3] = {1, 2, 2};
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      double acc = 0.0;
+    for (int q = 0; q < 3; ++q) {
+      const int i = PI[q], j = PJ[q];
+      double inner[7];
 #pragma unroll
-      for (int k = 0; k < 7; ++k) acc = tap(acc, W.w2[a][k], t[c + (k - 3) * st[a]]);
-      out[(long long)d2slot(f, sym(a, a)) * n] = acc;
+      for (int b = 0; b < 7; ++b) inner[b] = b == 3 ? 0.0 : c1_at(t + c + (b - 3) * st[j], st[i]);
+      out[(long long)d2slot(f, sym(i, j)) * n] =
+          __dmul_rn(c1_sum(inner[0], inner[1], inner[2], inner[4], inner[5], inner[6]), W.fm[q]);
     }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = i + 1; j < 3; ++j) {
-        double acc = 0.0;
-#pragma unroll
-        for (int b = 0; b < 7; ++b) {
-          if (b == 3) continue;
-          double inner = 0.0;
-#pragma unroll
-          for (int a = 0; a < 7; ++a)
-            if (a != 3) inner = tap(inner, W.w1[i][a], t[c + (a - 3) * st[i] + (b - 3) * st[j]]);
-          acc = tap(acc, W.w1[j][b], inner);
-        }
-        out[(long long)d2slot(f, sym(i, j)) * n] = acc;
-      }
   }
-  if (ko) {
-    double acc = 0.0;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 0; k <= 2 * R; ++k) s = tap(s, W.wko[a][k], t[c + (k - R) * st[a]]);
-      acc = __dadd_rn(acc, s);
-    }
-    out[(long long)(NDERIV + f) * n] = acc;
-  }
+  if (ko) out[(long long)(NDERIV + f) * n] = kacc;
 }
 
 template <int R>

@@ -15,10 +15,10 @@
 // constraints.
 //
 // Stencils follow 3D/src/bssn3d/derivative_bundle.py:31-48 and
-// common/src/mcs_common/derivatives.py:78-106: pre-scaled taps summed from
-// the lowest offset, index clamped at the array ends, mixed second
-// derivatives as a first derivative along the lower axis, then along the
-// higher axis of that result.
+// common/src/mcs_common/derivatives.py:35-106: the centred sixth-order
+// coefficients (integer sums of paired taps, scaled once), index clamped at
+// the array ends, mixed second derivatives as a first derivative along the
+// lower axis, then along the higher axis of that result.
 //
 // This header holds the stream kernel template and its host launch template;
 // its instantiations are spread over the stream_*.cu translation units
@@ -82,20 +82,43 @@ struct Args {
   double ctime;       // MSRK: this stage's node (stage time t + ctime * dt)
 };
 
-// Stencil weights, pre-scaled on the device from S like derivatives.py:78-81:
-// (coefficient / denominator) * factor, factor = 1/h, 1/h^2, sigma/h.
+// Stencil scale factors, set on the device from the grid spacing (per block
+// for block lists). Every stencil is summed with the integer coefficients of
+// common/src/mcs_common/derivatives.py:35-49 and scaled once:
+//   f1 = 1 / (60 h)           first derivative
+//   f2 = 1 / (180 h h)        diagonal second derivative
+//   fk = sigma / (64 h)       Kreiss-Oliger, order 6 (sigma / (256 h) for order 8)
+//   fm = f1_i * f1_j          mixed second derivative, pairs xy, xz, yz
 struct Weights {
-  double w1[3][7];
-  double w2[3][7];
-  double wko[3][9];
+  double f1[3], f2[3], fk[3], fm[3];
 };
 
-// Stencil sums are evaluated tap by tap from the lowest offset
-// (derivatives.py:78-88), each tap one fused multiply-add, the contraction the
-// reference's own CUDA kernel is compiled with. IEEE fma is exactly rounded,
-// so the CPU oracle (which uses fma() in the same order) reproduces every
-// derivative bit for bit.
-__device__ __forceinline__ double tap(double acc, double w, double v) { return __fma_rn(w, v, acc); }
+// Stencil sums. The symmetric taps are paired first (v[+k] - v[-k] for the
+// first derivative, v[+k] + v[-k] for the even stencils; the KO sum shares
+// the second derivative's pairs), then combined with the integer coefficients
+// from the outermost pair inwards, each step one fused multiply-add; the
+// caller applies the scale factor. The reference forms sum_k (c_k / den *
+// factor) * v_k (derivatives.py:78-88); the two orders differ by rounding
+// only. The CPU oracle evaluates the same operations in the same order, so
+// the derivatives match it bit for bit. v points at the centre tap, st is the
+// tap stride.
+__device__ __forceinline__ double c1_sum(double m3, double m2, double m1, double p1, double p2, double p3) {
+  const double a1 = __dsub_rn(p1, m1), a2 = __dsub_rn(p2, m2), a3 = __dsub_rn(p3, m3);
+  return __fma_rn(45.0, a1, __fma_rn(-9.0, a2, a3));
+}
+__device__ __forceinline__ double c2_sum(double v0, double s1, double s2, double s3) {
+  return __fma_rn(-490.0, v0, __fma_rn(270.0, s1, __fma_rn(-27.0, s2, __dadd_rn(s3, s3))));
+}
+__device__ __forceinline__ double ko6_sum(double v0, double s1, double s2, double s3) {
+  return __fma_rn(-20.0, v0, __fma_rn(15.0, s1, __fma_rn(-6.0, s2, s3)));
+}
+__device__ __forceinline__ double ko8_sum(double v0, double s1, double s2, double s3, double s4) {
+  return __fma_rn(-70.0, v0, __fma_rn(56.0, s1, __fma_rn(-28.0, s2, __fma_rn(8.0, s3, -s4))));
+}
+// first-derivative sum of the 7 taps around p (stride st)
+__device__ __forceinline__ double c1_at(const double* p, int st) {
+  return c1_sum(p[-3 * st], p[-2 * st], p[-st], p[st], p[2 * st], p[3 * st]);
+}
 
 __device__ __forceinline__ long long clampll(long long v, long long hi) {
   return v < 0 ? 0 : (v > hi ? hi : v);
@@ -220,31 +243,23 @@ __device__ __forceinline__ Params load_params(const double* __restrict__ S) {
   return P;
 }
 
+// The scale factors of one grid or block: thread a < 3 sets axis a and the
+// mixed pair a (xy, xz, yz) from the three spacings h.
 template <int R>
-__device__ __forceinline__ void init_weights(Weights& W, const double* __restrict__ S, double ko_sigma, int tid);
-
-// One axis of the weights from that axis' spacing (batched blocks carry their own).
-template <int R>
-__device__ __forceinline__ void init_weights_h(Weights& W, double h, double ko_sigma, int a) {
-  const double c1[7] = {-1, 9, -45, 0, 45, -9, 1};
-  const double c2[7] = {2, -27, 270, -490, 270, -27, 2};
-  const double k6[7] = {1, -6, 15, -20, 15, -6, 1};
-  const double k8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1};
-  const double f1 = 1.0 / h, f2 = 1.0 / (h * h), fk = ko_sigma / h;
-  for (int k = 0; k < 7; ++k) {
-    W.w1[a][k] = (c1[k] / 60.0) * f1;
-    W.w2[a][k] = (c2[k] / 180.0) * f2;
-  }
-  for (int k = 0; k < 9; ++k) W.wko[a][k] = 0.0;
-  if (R == 4)
-    for (int k = 0; k < 9; ++k) W.wko[a][k] = (k8[k] / 256.0) * fk;
-  else
-    for (int k = 0; k < 7; ++k) W.wko[a][k] = (k6[k] / 64.0) * fk;
+__device__ __forceinline__ void init_weights_h(Weights& W, const double* h, double ko_sigma, int a) {
+  constexpr int PI[3] = {0, 0, 1}, PJ[3] = {1, 2, 2};
+  W.f1[a] = 1.0 / (60.0 * h[a]);
+  W.f2[a] = 1.0 / ((180.0 * h[a]) * h[a]);
+  W.fk[a] = ko_sigma / ((R == 4 ? 256.0 : 64.0) * h[a]);
+  W.fm[a] = (1.0 / (60.0 * h[PI[a]])) * (1.0 / (60.0 * h[PJ[a]]));
 }
 
 template <int R>
 __device__ __forceinline__ void init_weights(Weights& W, const double* __restrict__ S, double ko_sigma, int tid) {
-  if (tid < 3) init_weights_h<R>(W, S[13 + tid], ko_sigma, tid);
+  if (tid < 3) {
+    const double h[3] = {S[13], S[14], S[15]};
+    init_weights_h<R>(W, h, ko_sigma, tid);
+  }
 }
 
 // Issue the cp.async copies that stage one field's haloed tile, index clamped
@@ -401,7 +416,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       if (lo != cur_block) {
         // every thread must be done with the previous tile's last field step
         if (NEWPIPE) __syncthreads();
-        if (tid < 3) init_weights_h<R>(W, bk.h[tid], args.ko_sigma, tid);
+        if (tid < 3) init_weights_h<R>(W, bk.h, args.ko_sigma, tid);
         cur_block = lo;
       }
     }
@@ -532,60 +547,40 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         double v[2 * R + 1];
 #pragma unroll
         for (int k = 0; k <= 2 * R; ++k) v[k] = cur[c + (k - R) * st[a]];
-        double s1 = 0.0;
-#pragma unroll
-        for (int k = 0; k < 7; ++k)
-          if (k != 3) s1 = tap(s1, W.w1[a][k], v[k + R - 3]);
-        d1[a] = s1;
-        if (has_d2(f)) {
-          double s2 = 0.0;
-#pragma unroll
-          for (int k = 0; k < 7; ++k) s2 = tap(s2, W.w2[a][k], v[k + R - 3]);
-          d2[sym(a, a)] = s2;
-        }
+        d1[a] = __dmul_rn(c1_sum(v[R - 3], v[R - 2], v[R - 1], v[R + 1], v[R + 2], v[R + 3]), W.f1[a]);
+        const double s1 = __dadd_rn(v[R + 1], v[R - 1]), s2 = __dadd_rn(v[R + 2], v[R - 2]),
+                     s3 = __dadd_rn(v[R + 3], v[R - 3]);
+        if (has_d2(f)) d2[sym(a, a)] = __dmul_rn(c2_sum(v[R], s1, s2, s3), W.f2[a]);
         if (use_ko) {
-          double sk = 0.0;
-#pragma unroll
-          for (int k = 0; k <= 2 * R; ++k) sk = tap(sk, W.wko[a][k], v[k]);
-          ko = __dadd_rn(ko, sk);
+          const double sk = R == 4 ? ko8_sum(v[R], s1, s2, s3, __dadd_rn(v[2 * R], v[0])) : ko6_sum(v[R], s1, s2, s3);
+          ko = __dadd_rn(ko, __dmul_rn(sk, W.fk[a]));
         }
       }
       if (has_d2(f)) {
-        // T1 = d/dx over x in [0,TX), y in [-3, TY+3), z in [-3, TZ+3)
+        // T1 = unscaled d/dx sums over x in [0,TX), y in [-3, TY+3), z in [-3, TZ+3)
         for (int e = tid; e < T1N; e += NTHREADS) {
           const int zz = e % TROW;
           const int yy = (e / TROW) % Geo::T1Y;
           const int xx = e / (TROW * Geo::T1Y);
           const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R + ZS);
-          double s = 0.0;
-#pragma unroll
-          for (int k = 0; k < 7; ++k)
-            if (k != 3) s = tap(s, W.w1[0][k], cur[cc + (k - 3) * Geo::SX]);
+          const double s = c1_at(cur + cc, Geo::SX);
           T1[(xx * Geo::T1Y + yy) * HZP + zz] = s;
         }
-        // T2 = d/dy over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
+        // T2 = unscaled d/dy sums over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
         for (int e = tid; e < T2N; e += NTHREADS) {
           const int zz = e % TROW;
           const int yy = (e / TROW) % TY;
           const int xx = e / (TROW * TY);
           const int cc = (xx + R) * Geo::SX + (yy + R) * Geo::SY + (zz - 3 + R + ZS);
-          double s = 0.0;
-#pragma unroll
-          for (int k = 0; k < 7; ++k)
-            if (k != 3) s = tap(s, W.w1[1][k], cur[cc + (k - 3) * Geo::SY]);
+          const double s = c1_at(cur + cc, Geo::SY);
           T2[(xx * TY + yy) * HZP + zz] = s;
         }
         __syncthreads();
-        double sxy = 0.0, sxz = 0.0, syz = 0.0;
         const int t1c = (lx * Geo::T1Y + ly + 3) * HZP + lz + 3;
         const int t2c = (lx * TY + ly) * HZP + lz + 3;
-#pragma unroll
-        for (int k = 0; k < 7; ++k) {
-          if (k == 3) continue;
-          sxy = tap(sxy, W.w1[1][k], T1[t1c + (k - 3) * HZP]);
-          sxz = tap(sxz, W.w1[2][k], T1[t1c + (k - 3)]);
-          syz = tap(syz, W.w1[2][k], T2[t2c + (k - 3)]);
-        }
+        const double sxy = __dmul_rn(c1_at(T1 + t1c, HZP), W.fm[0]);
+        const double sxz = __dmul_rn(c1_at(T1 + t1c, 1), W.fm[1]);
+        const double syz = __dmul_rn(c1_at(T2 + t2c, 1), W.fm[2]);
         d2[sym(0, 1)] = sxy;
         d2[sym(0, 2)] = sxz;
         d2[sym(1, 2)] = syz;

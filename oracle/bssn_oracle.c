@@ -9,7 +9,7 @@
  *   - centred 6th-order first/second-derivative stencils and the 6th/8th-order
  *     Kreiss-Oliger stencils with edge padding by the stencil's own reach
  *       common/src/mcs_common/derivatives.py:35-49 (coefficients),
- *       derivatives.py:78-88 (_apply: pre-scaled taps, edge pad, tap order)
+ *       derivatives.py:78-88 (_apply: edge pad by the stencil's reach)
  *   - the 138-derivative bundle (mixed second derivative = first derivative
  *     along the lower axis, then along the higher one)
  *       3D/src/bssn3d/derivative_bundle.py:31-48
@@ -55,26 +55,42 @@ int oracle_g2_slot(int field) {
 /* stencils                                                            */
 /* ------------------------------------------------------------------ */
 
-static const double C1_6[7] = {-1, 9, -45, 0, 45, -9, 1};       /* /60  */
-static const double C2_6[7] = {2, -27, 270, -490, 270, -27, 2}; /* /180 */
-static const double KO_6[7] = {1, -6, 15, -20, 15, -6, 1};      /* /64  */
-static const double KO_8[9] = {-1, 8, -28, 56, -70, 56, -28, 8, -1}; /* /256 */
+/* Stencil kinds. Every stencil is the integer-coefficient sum of
+ * common/src/mcs_common/derivatives.py:35-49 over the taps in[clamp(p + k)],
+ * symmetric taps paired first and combined from the outermost pair inwards
+ * with fused multiply-adds, then scaled once:
+ *   C1  45 (v1 - v-1) - 9 (v2 - v-2) + (v3 - v-3)                   / 60
+ *   C2  -490 v0 + 270 (v1 + v-1) - 27 (v2 + v-2) + 2 (v3 + v-3)      / 180
+ *   KO6 -20 v0 + 15 (v1 + v-1) - 6 (v2 + v-2) + (v3 + v-3)          / 64
+ *   KO8 -70 v0 + 56 (v1 + v-1) - 28 (v2 + v-2) + 8 (v3 + v-3) - (v4 + v-4)  / 256
+ * The reference sums (c_k / den * factor) * v_k in tap order
+ * (derivatives.py:78-88); the two differ by rounding only. The GPU kernels
+ * evaluate exactly these operations in this order, so their derivatives equal
+ * this restatement bit for bit. */
+enum { ST_C1 = 0, ST_C2 = 1, ST_KO6 = 2, ST_KO8 = 3 };
 
 static inline long clampl(long v, long lo, long hi) {
   return v < lo ? lo : (v > hi ? hi : v);
 }
 
-/* One pass of a centred stencil along `axis` of a (Sx,Sy,Sz) array:
- * out = sum_k (coef[k]/den*factor) * in[clamp(p + k - reach)], summed in tap
- * order from the lowest offset, like derivatives.py:78-88, each tap one fused
- * multiply-add (the contraction the reference's CUDA kernel is compiled with,
- * 3D/src/bssn3d/cuda/rhs_fused.cu; IEEE fma is exactly rounded, so the GPU
- * taps reproduce these values bit for bit). */
-static void apply_axis(const double* in, double* out, const long S[3], int axis,
-                       const double* coef, int ntap, double den, double factor) {
-  const int reach = (ntap - 1) / 2;
-  double w[9];
-  for (int k = 0; k < ntap; ++k) w[k] = (coef[k] / den) * factor;
+static double stencil_sum(int kind, const double* v /* centre tap, v[-4..4] */) {
+  if (kind == ST_C1) {
+    const double a1 = v[1] - v[-1], a2 = v[2] - v[-2], a3 = v[3] - v[-3];
+    return fma(45.0, a1, fma(-9.0, a2, a3));
+  }
+  const double s1 = v[1] + v[-1], s2 = v[2] + v[-2], s3 = v[3] + v[-3];
+  if (kind == ST_C2) return fma(-490.0, v[0], fma(270.0, s1, fma(-27.0, s2, s3 + s3)));
+  if (kind == ST_KO6) return fma(-20.0, v[0], fma(15.0, s1, fma(-6.0, s2, s3)));
+  const double s4 = v[4] + v[-4];
+  return fma(-70.0, v[0], fma(56.0, s1, fma(-28.0, s2, fma(8.0, s3, -s4))));
+}
+
+/* One pass of a centred stencil along `axis` of a (Sx,Sy,Sz) array, edge
+ * padded by clamping the tap index (derivatives.py:83-84):
+ * out = stencil_sum * scale, or the unscaled sum when scaled == 0. */
+static void apply_axis(const double* in, double* out, const long S[3], int axis, int kind,
+                       int scaled, double scale) {
+  const int reach = kind == ST_KO8 ? 4 : 3;
   const long Sx = S[0], Sy = S[1], Sz = S[2];
   const long stride[3] = {Sy * Sz, Sz, 1};
 #pragma omp parallel for collapse(2) schedule(static)
@@ -85,14 +101,18 @@ static void apply_axis(const double* in, double* out, const long S[3], int axis,
         const long base = x * stride[0] + y * stride[1] + z;
         const long pa = p[axis];
         const long off0 = base - pa * stride[axis];
-        double acc = 0.0;
-        for (int k = 0; k < ntap; ++k) {
-          long q = clampl(pa + k - reach, 0, S[axis] - 1);
-          acc = fma(w[k], in[off0 + q * stride[axis]], acc);
-        }
-        out[base] = acc;
+        double v[9];
+        for (int k = -reach; k <= reach; ++k)
+          v[4 + k] = in[off0 + clampl(pa + k, 0, S[axis] - 1) * stride[axis]];
+        const double sum = stencil_sum(kind, v + 4);
+        out[base] = scaled ? sum * scale : sum;
       }
 }
+
+/* scale factors of the stencils on spacing h (the GPU kernels form them with
+ * the same operations) */
+static double f1_of(double h) { return 1.0 / (60.0 * h); }
+static double f2_of(double h) { return 1.0 / ((180.0 * h) * h); }
 
 /* The 138 derivatives of a (24,Sx,Sy,Sz) state. D is [138][n]. */
 void oracle_derivatives(const double* F, long Sx, long Sy, long Sz, double dx,
@@ -103,18 +123,17 @@ void oracle_derivatives(const double* F, long Sx, long Sy, long Sz, double dx,
   double* tmp = (double*)malloc(sizeof(double) * n);
   for (int f = 0; f < NF; ++f)
     for (int a = 0; a < 3; ++a)
-      apply_axis(F + f * n, D + (long)(3 * f + a) * n, S, a, C1_6, 7, 60.0,
-                 1.0 / h[a]);
+      apply_axis(F + f * n, D + (long)(3 * f + a) * n, S, a, ST_C1, 1, f1_of(h[a]));
   for (int m = 0; m < 11; ++m) {
     const double* u = F + (long)G2FIELDS[m] * n;
     for (int p = 0; p < 6; ++p) {
       const int i = SYM_I[p], j = SYM_J[p];
       double* out = D + (long)(72 + 6 * m + p) * n;
       if (i == j) {
-        apply_axis(u, out, S, i, C2_6, 7, 180.0, 1.0 / (h[i] * h[i]));
+        apply_axis(u, out, S, i, ST_C2, 1, f2_of(h[i]));
       } else {
-        apply_axis(u, tmp, S, i, C1_6, 7, 60.0, 1.0 / h[i]);
-        apply_axis(tmp, out, S, j, C1_6, 7, 60.0, 1.0 / h[j]);
+        apply_axis(u, tmp, S, i, ST_C1, 0, 0.0);
+        apply_axis(tmp, out, S, j, ST_C1, 1, f1_of(h[i]) * f1_of(h[j]));
       }
     }
   }
@@ -129,14 +148,13 @@ void oracle_ko(const double* F, long Sx, long Sy, long Sz, double dx, double dy,
   const long n = Sx * Sy * Sz;
   const double h[3] = {dx, dy, dz};
   double* tmp = (double*)malloc(sizeof(double) * n);
-  const double* coef = ko_order == 8 ? KO_8 : KO_6;
-  const int ntap = ko_order == 8 ? 9 : 7;
+  const int kind = ko_order == 8 ? ST_KO8 : ST_KO6;
   const double den = ko_order == 8 ? 256.0 : 64.0;
   for (int f = 0; f < NF; ++f) {
     double* acc = KO + (long)f * n;
     for (long q = 0; q < n; ++q) acc[q] = 0.0;
     for (int a = 0; a < 3; ++a) {
-      apply_axis(F + (long)f * n, tmp, S, a, coef, ntap, den, sigma / h[a]);
+      apply_axis(F + (long)f * n, tmp, S, a, kind, 1, sigma / (den * h[a]));
       for (long q = 0; q < n; ++q) acc[q] = acc[q] + tmp[q];
     }
   }
