@@ -230,7 +230,7 @@ struct TileGeom {
   // shared memory they take comes out of the L1 that holds the register
   // spills: measured 2-6 % slower on B200, so the staging rotates two.
   static constexpr int NBUF = 2;
-  static constexpr size_t SMEM_RUN = SMEM + SMEM_PTS + (NBUF == 3 ? (size_t)VOL * sizeof(double) : 0);
+  static constexpr size_t SMEM_RUN = SMEM + SMEM_PTS;
 };
 
 __device__ __forceinline__ Params load_params(const double* __restrict__ S) {
@@ -349,13 +349,12 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
   double* const pA = pU + NFIELD * NTHREADS;  // [24][256] accumulator (stages 1-3)
   __shared__ Weights W;
   __shared__ __align__(8) unsigned long long tbar[3];  // bulk-copy completion, one per buffer
-  // per-thread staging: the next field's copies are issued after the
-  // field-start barrier, which then also frees the previous field's buffer and
-  // T1/T2, so the field step needs no closing barrier
+  // the next field's copies are issued after the field-start barrier, which
+  // then also frees the previous field's buffer and T1/T2, so the field step
+  // needs no closing barrier
   constexpr int NB = Geo::NBUF;
-  constexpr bool NEWPIPE = !TMA;
-  double* const buf2 = T2 + Geo::T2VOL + (Geo::PTS ? 3 * NFIELD * NTHREADS : 0);  // used when NBUF is 3
-  auto bufp = [&](int b) -> double* { return b == 0 ? buf0 : (b == 1 ? buf1 : buf2); };
+  static_assert(NB == 2, "the staging pipeline rotates two buffers");
+  auto bufp = [&](int b) -> double* { return b == 0 ? buf0 : buf1; };
 
   const int tid = threadIdx.x;
   const bool batched = args.blocks != nullptr;
@@ -415,7 +414,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       P.dx = bk.h[0]; P.hx = bk.h[0]; P.hy = bk.h[1]; P.hz = bk.h[2];
       if (lo != cur_block) {
         // every thread must be done with the previous tile's last field step
-        if (NEWPIPE) __syncthreads();
+        __syncthreads();
         if (tid < 3) init_weights_h<R>(W, bk.h, args.ko_sigma, tid);
         cur_block = lo;
       }
@@ -484,22 +483,20 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         const double* src = buf + (cx - bx0) * Geo::SX + (cy - by0) * Geo::SY;
         const int zlo = bz0 < 0 ? -bz0 : 0;                                       // first in-array cell
         const int zhi = bz0 + Geo::BOXZ > Sz ? (int)Sz - bz0 : Geo::BOXZ;          // one past the last
-        const bool whole = cx != X || cy != Y;
-        for (int hz = 0; hz < Geo::BOXZ; ++hz) {
-          const int q = hz < zlo ? zlo : (hz >= zhi ? zhi - 1 : hz);
-          if (whole || q != hz) dst[hz] = src[q];
+        if (cx != X || cy != Y) {
+          for (int hz = 0; hz < Geo::BOXZ; ++hz) dst[hz] = src[hz < zlo ? zlo : (hz >= zhi ? zhi - 1 : hz)];
+        } else {
+          for (int hz = 0; hz < zlo; ++hz) dst[hz] = src[zlo];
+          for (int hz = zhi; hz < Geo::BOXZ; ++hz) dst[hz] = src[zhi - 1];
         }
       }
     };
+    // the first field's copies; later fields are issued one step ahead, right
+    // after the barrier that frees their buffer
     if (TMA) {
-      for (int q = 0; q < NB - 1; ++q) tma_issue(stream_field(q), q);
-    } else if (NEWPIPE) {
-      for (int q = 0; q < NB - 1; ++q) {
-        stage_tile<R, T, ZS>(bufp(q), Fbase + (long long)stream_field(q) * n, x0, y0, z0, Sx, Sy, Sz, tid);
-        cp_async_commit();
-      }
+      tma_issue(stream_field(0), 0);
     } else {
-      stage_tile<R, T, ZS>(buf0, Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
+      stage_tile<R, T, ZS>(bufp(0), Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
       cp_async_commit();
     }
     Unroll<0, NFIELD>::run([&](auto ic) {
@@ -507,9 +504,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       constexpr int f = stream_field(idx);
       constexpr int b = idx % NB;
       const double* __restrict__ cur = bufp(b);
+      // One barrier per field step: field idx's tile has landed (and, for
+      // bulk copies on an edge tile, been clamped) everywhere, and every
+      // thread is done with field idx - 1, whose buffer and T1/T2 are then
+      // free for the next field's copies.
       if (TMA) {
-        // the buffer of field idx - 1 is free (the field step ended in a barrier)
-        if (idx + NB - 1 < NFIELD) tma_issue(stream_field(idx + NB - 1), (idx + NB - 1) % NB);
         if (idx == NFIELD - 1) cp_async_wait<0>();  // the point staging of u_n / accumulator
         if (!tfailed && mbar_wait_bounded(&tbar[b], (tphase >> b) & 1u)) tpending &= ~(1u << b);
         else tfailed = true;  // results of this CTA are garbage; the error count says so
@@ -517,27 +516,17 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         if (edge) {
           clamp_box(bufp(b));
           fence_proxy_async();  // these writes before the next bulk copy into the buffer
-          __syncthreads();
         }
-      } else if (NEWPIPE) {
-        constexpr int PEND = NB - 2 < NFIELD - 1 - idx ? NB - 2 : NFIELD - 1 - idx;  // fields issued after idx
-        cp_async_wait<PEND>();
         __syncthreads();
-        if (idx + NB - 1 < NFIELD) {
-          stage_tile<R, T, ZS>(bufp((idx + NB - 1) % NB), Fbase + (long long)stream_field(idx + NB - 1) * n, x0,
-                               y0, z0, Sx, Sy, Sz, tid);
-          cp_async_commit();
-        }
+        if (idx + 1 < NFIELD) tma_issue(stream_field(idx + 1), (idx + 1) % NB);
       } else {
-        if (idx + 1 < NFIELD) {
-          stage_tile<R, T, ZS>((idx & 1) ? buf0 : buf1, Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
-                           Sx, Sy, Sz, tid);
-          cp_async_commit();
-          cp_async_wait<1>();
-        } else {
-          cp_async_wait<0>();
-        }
+        cp_async_wait<0>();
         __syncthreads();
+        if (idx + 1 < NFIELD) {
+          stage_tile<R, T, ZS>(bufp((idx + 1) % NB), Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
+                               Sx, Sy, Sz, tid);
+          cp_async_commit();
+        }
       }
 
       // axial taps: first derivative, diagonal second derivative, KO
@@ -589,7 +578,6 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         for (int p = 0; p < 6; ++p) d2[p] = 0.0;
       }
       acc.consume(f, d1, d2, ko, P, fld);
-      if (!NEWPIPE) __syncthreads();  // staged buffer and T1/T2 are reused
     });
 
     // ---- epilogue ---------------------------------------------------------
