@@ -2,6 +2,8 @@
 
     python integer-schemes_b200/build.py          # libbssn_b200.so (+ -Xptxas -v report)
 
+Extra nvcc flags (e.g. -DBSSN_B200_NO_TMA) can be given in $BSSN_B200_NVCC_FLAGS.
+
 The library lands next to the Python package that loads it
 (``bssn3d_b200/libbssn_b200.so``), so it travels with the source tree.
 """
@@ -54,6 +56,7 @@ def _compile(src: Path) -> tuple:
     obj = OBJ_DIR / (src.stem + ".o")
     cmd = [nvcc(), *ARCH, *host_compiler(), "-O3", "-lineinfo", "-std=c++17",
            "-Xptxas", "-v", "-Xcompiler", "-fPIC", "-diag-suppress", "177",
+           *os.environ.get("BSSN_B200_NVCC_FLAGS", "").split(),
            "-c", str(src), "-o", str(obj)]
     proc = subprocess.run(cmd, capture_output=True, text=True)
     return src, obj, proc

@@ -704,6 +704,9 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
 }  // namespace bssn
 
 namespace bssn_host {
+// Internal linkage for everything below: each translation unit keeps its own
+// per-device flags, and two loaded copies of the library never share them.
+namespace {
 
 // Opt a kernel into its dynamic shared memory once per device.
 template <class K>
@@ -725,7 +728,7 @@ using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, 
                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-inline EncodeTiled encode_tiled() {
+EncodeTiled encode_tiled() {
   static EncodeTiled fn = [] {
     void* p = nullptr;
     cudaDriverEntryPointQueryResult q;
@@ -768,7 +771,7 @@ bool make_state_map(CUtensorMap* map, const double* F, long long Sx, long long S
 // reads its environment knobs (3D/src/bssn3d/cuda/rhs_fused.cu:34-41). Both
 // give the same bytes; on B200 the per-thread form measured faster for this
 // kernel (its warps stay in step through the unrolled field loop).
-inline bool tma_staging_requested() {
+bool tma_staging_requested() {
   const char* v = std::getenv("BSSN_B200_STAGING");
   return v != nullptr && std::strcmp(v, "tma") == 0;
 }
@@ -802,9 +805,8 @@ int launch_stream(const bssn::Args& a, cudaStream_t stream, int grid) {
   return 0;
 }
 
-// Reads this translation unit's bulk-copy error counter (internal linkage:
-// every translation unit reads its own).
-static int read_copy_errors(int* count) {
+// Reads this translation unit's bulk-copy error counter.
+int read_copy_errors(int* count) {
   int v = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&v, bssn::g_async_copy_errors, sizeof(int));
   if (e != cudaSuccess) return cuda_fail("async_copy_errors", e);
@@ -812,4 +814,5 @@ static int read_copy_errors(int* count) {
   return 0;
 }
 
+}  // namespace
 }  // namespace bssn_host
