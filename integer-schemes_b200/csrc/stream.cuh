@@ -82,11 +82,21 @@ struct NoCon {
   __device__ __forceinline__ void operator()(double, double, double, double) const {}
 };
 
-template <bool RATES, bool CONS>
+template <bool RATES, bool CONS, bool PV = false>
 struct Stream {
-  // point values kept in registers
-  double al, chi, ichi, K;
-  double g[6], gu[6], b[3];
+  // Point values: held in registers, or (PV) re-read on every use from the
+  // point's staged column pv[k * ps] (shared memory), which frees their
+  // registers for the accumulators.
+  const double* pv = nullptr;
+  int ps = 0;
+  double al_, chi_, K_, g_[6], b_[3];
+  __device__ __forceinline__ double Al() const { return PV ? pv[F_ALPHA * ps] : al_; }
+  __device__ __forceinline__ double Chi() const { return PV ? pv[F_CHI * ps] : chi_; }
+  __device__ __forceinline__ double Kv() const { return PV ? pv[F_K * ps] : K_; }
+  __device__ __forceinline__ double Gv(int p) const { return PV ? pv[(F_GT + p) * ps] : g_[p]; }
+  __device__ __forceinline__ double Bv(int i) const { return PV ? pv[(F_BETA + i) * ps] : b_[i]; }
+  double ichi;
+  double gu[6];
   double AU[6], AA;
   // rates
   double r_gt[6], r_At[6], r_Gt[3], ko_Gt[3], r_beta[3], r_B[3], r_alpha, r_chi, r_K;
@@ -101,22 +111,24 @@ struct Stream {
 
   template <class Fld>
   __device__ __forceinline__ void init(const Fld& fld) {
-    al = fld(F_ALPHA);
-    chi = fld(F_CHI);
-    ichi = 1.0 / chi;
-    K = fld(F_K);
+    if (!PV) {
+      al_ = fld(F_ALPHA);
+      chi_ = fld(F_CHI);
+      K_ = fld(F_K);
 #pragma unroll
-    for (int p = 0; p < 6; ++p) g[p] = fld(F_GT + p);
+      for (int p = 0; p < 6; ++p) g_[p] = fld(F_GT + p);
 #pragma unroll
-    for (int i = 0; i < 3; ++i) b[i] = fld(F_BETA + i);
+      for (int i = 0; i < 3; ++i) b_[i] = fld(F_BETA + i);
+    }
+    ichi = 1.0 / Chi();
     {
-      const double a00 = g[3] * g[5] - g[4] * g[4];
-      const double a01 = g[2] * g[4] - g[1] * g[5];
-      const double a02 = g[1] * g[4] - g[2] * g[3];
-      const double a11 = g[0] * g[5] - g[2] * g[2];
-      const double a12 = g[1] * g[2] - g[0] * g[4];
-      const double a22 = g[0] * g[3] - g[1] * g[1];
-      const double idet = 1.0 / (g[0] * a00 + g[1] * a01 + g[2] * a02);
+      const double a00 = Gv(3) * Gv(5) - Gv(4) * Gv(4);
+      const double a01 = Gv(2) * Gv(4) - Gv(1) * Gv(5);
+      const double a02 = Gv(1) * Gv(4) - Gv(2) * Gv(3);
+      const double a11 = Gv(0) * Gv(5) - Gv(2) * Gv(2);
+      const double a12 = Gv(1) * Gv(2) - Gv(0) * Gv(4);
+      const double a22 = Gv(0) * Gv(3) - Gv(1) * Gv(1);
+      const double idet = 1.0 / (Gv(0) * a00 + Gv(1) * a01 + Gv(2) * a02);
       gu[0] = a00 * idet; gu[1] = a01 * idet; gu[2] = a02 * idet;
       gu[3] = a11 * idet; gu[4] = a12 * idet; gu[5] = a22 * idet;
     }
@@ -146,7 +158,7 @@ struct Stream {
   }
 
   __device__ __forceinline__ double adv(const double (&d1)[3]) const {
-    return b[0] * d1[0] + b[1] * d1[1] + b[2] * d1[2];
+    return Bv(0) * d1[0] + Bv(1) * d1[1] + Bv(2) * d1[2];
   }
 
   // ---- gt_p: first derivatives kept, second derivatives into R_p ------------
@@ -212,12 +224,12 @@ struct Stream {
         double c2au = 0.0;
 #pragma unroll
         for (int p = 0; p < 6; ++p) c2au += symw(p) * C2[i][p] * AU[p];
-        r_Gt[i] += 2.0 * al * c2au;
+        r_Gt[i] += 2.0 * Al() * c2au;
       }
     }
   }
 
-  // ---- chi --------------------------------------------------------------------
+  // ---- chi ----------------------------------------------------------------------
   __device__ __forceinline__ void consume_chi(const double (&d1)[3], const double (&d2)[6], double ko) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) dchi[a] = d1[a];
@@ -236,13 +248,13 @@ struct Stream {
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
       const int i = sym_i(p), j = sym_j(p);
-      R[p] += hichi * (Dchi[p] + g[p] * lapchi) - qichi2 * (dchi[i] * dchi[j] + 3.0 * g[p] * sqchi);
+      R[p] += hichi * (Dchi[p] + Gv(p) * lapchi) - qichi2 * (dchi[i] * dchi[j] + 3.0 * Gv(p) * sqchi);
     }
     if (RATES) {
 #pragma unroll
       for (int i = 0; i < 3; ++i) {
         const double t = AU[sym(i, 0)] * dchi[0] + AU[sym(i, 1)] * dchi[1] + AU[sym(i, 2)] * dchi[2];
-        r_Gt[i] -= 3.0 * al * ichi * t;
+        r_Gt[i] -= 3.0 * Al() * ichi * t;
       }
     }
   }
@@ -257,7 +269,7 @@ struct Stream {
     for (int p = 0; p < 6; ++p) {
       const int i = sym_i(p), j = sym_j(p);
       const double dda = d2[p] - (C2[0][p] * dal[0] + C2[1][p] * dal[1] + C2[2][p] * dal[2]) +
-                         hichi * (dal[i] * dchi[j] + dal[j] * dchi[i] - g[p] * gchial);
+                         hichi * (dal[i] * dchi[j] + dal[j] * dchi[i] - Gv(p) * gchial);
       X[p] = -dda;
       lapa += symw(p) * gu[p] * dda;
     }
@@ -277,7 +289,7 @@ struct Stream {
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
       const int i = sym_i(p), j = sym_j(p);
-      R[p] += 0.5 * (g[sym(k, i)] * d1[j] + g[sym(k, j)] * d1[i]);
+      R[p] += 0.5 * (Gv(sym(k, i)) * d1[j] + Gv(sym(k, j)) * d1[i]);
     }
   }
 
@@ -286,7 +298,7 @@ struct Stream {
     trX = 0.0;
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
-      X[p] += al * R[p];
+      X[p] += Al() * R[p];
       trR += symw(p) * gu[p] * R[p];
       trX += symw(p) * gu[p] * X[p];
     }
@@ -301,7 +313,7 @@ struct Stream {
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
       const int i = sym_i(p), j = sym_j(p);
-      r_gt[p] += g[sym(i, k)] * d1[j] + g[sym(j, k)] * d1[i];
+      r_gt[p] += Gv(sym(i, k)) * d1[j] + Gv(sym(j, k)) * d1[i];
       r_At[p] += fld(F_AT + sym(i, k)) * d1[j] + fld(F_AT + sym(j, k)) * d1[i];
     }
     double lapb = 0.0;
@@ -318,23 +330,23 @@ struct Stream {
 #pragma unroll
     for (int p = 0; p < 6; ++p) {
       const double A = fld(F_AT + p);
-      r_gt[p] += -t23 * g[p] * divb - 2.0 * al * A;
+      r_gt[p] += -t23 * Gv(p) * divb - 2.0 * Al() * A;
       r_At[p] += -t23 * A * divb;
     }
-    r_chi += t23 * chi * (al * K - divb);
+    r_chi += t23 * Chi() * (Al() * Kv() - divb);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
       r_Gt[i] += t23 * CalGt[i] * divb +
                  (1.0 / 3.0) * (gu[sym(i, 0)] * dd[0] + gu[sym(i, 1)] * dd[1] + gu[sym(i, 2)] * dd[2]);
   }
 
-  // ---- K ----------------------------------------------------------------------
+  // ---- K -------------------------------------------------------------------------
   __device__ __forceinline__ void consume_K(const double (&d1)[3], double ko) {
     r_K = adv(d1) + ko;
     if (RATES) {
 #pragma unroll
       for (int i = 0; i < 3; ++i)
-        r_Gt[i] -= (4.0 / 3.0) * al * (gu[sym(i, 0)] * d1[0] + gu[sym(i, 1)] * d1[1] + gu[sym(i, 2)] * d1[2]);
+        r_Gt[i] -= (4.0 / 3.0) * Al() * (gu[sym(i, 0)] * d1[0] + gu[sym(i, 1)] * d1[1] + gu[sym(i, 2)] * d1[2]);
     }
     if (CONS) {
 #pragma unroll
@@ -361,7 +373,7 @@ struct Stream {
   // ---- closing terms; emit(field, rate) and con(H, M0, M1, M2) ------------------------
   template <class Fld, class Emit, class Con>
   __device__ __forceinline__ void finalize(const Fld& fld, const Params& P, const Emit& emit, const Con& con) {
-    const double H = chi * trR + (2.0 / 3.0) * K * K - AA;
+    const double H = Chi() * trR + (2.0 / 3.0) * Kv() * Kv() - AA;
     if (CONS) {
       double A[6];
 #pragma unroll
@@ -399,20 +411,20 @@ struct Stream {
       for (int p = 0; p < 6; ++p) {
         const int i = sym_i(p), j = sym_j(p);
         const double aga = M[i][0] * A[sym(0, j)] + M[i][1] * A[sym(1, j)] + M[i][2] * A[sym(2, j)];
-        emit(F_AT + p, r_At[p] + chi * (X[p] - g[p] * third_trX) + al * (K * A[p] - 2.0 * aga));
+        emit(F_AT + p, r_At[p] + Chi() * (X[p] - Gv(p) * third_trX) + Al() * (Kv() * A[p] - 2.0 * aga));
       }
     }
-    emit(F_K, r_K - chi * lapa + al * (K * K * (1.0 / 3.0) + AA));
+    emit(F_K, r_K - Chi() * lapa + Al() * (Kv() * Kv() * (1.0 / 3.0) + AA));
     {
       const double dx2 = P.dx * P.dx;
-      emit(F_CHI, r_chi + P.cahd_c * dx2 * chi * H / (P.dt * (10.0 * dx2 + 1.0)));
+      emit(F_CHI, r_chi + P.cahd_c * dx2 * Chi() * H / (P.dt * (10.0 * dx2 + 1.0)));
     }
     {
-      const double sq = sqrt(chi);
-      emit(F_ALPHA, r_alpha - 2.0 * al * K -
-                        sq * P.ssl_h * (al - sq) * exp(-0.5 * P.t * P.t / (P.ssl_sigma * P.ssl_sigma)));
+      const double sq = sqrt(Chi());
+      emit(F_ALPHA, r_alpha - 2.0 * Al() * Kv() -
+                        sq * P.ssl_h * (Al() - sq) * exp(-0.5 * P.t * P.t / (P.ssl_sigma * P.ssl_sigma)));
     }
-    const double lf = 0.75 * (P.lamf0 + P.lamf1 * al);
+    const double lf = 0.75 * (P.lamf0 + P.lamf1 * Al());
 #pragma unroll
     for (int i = 0; i < 3; ++i) {
       const double Bi = fld(F_B + i);

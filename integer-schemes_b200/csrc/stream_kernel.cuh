@@ -452,7 +452,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       return Geo::PTS ? pY[k * NTHREADS + tid] : __ldg(Fp + (long long)k * n);
     };
 
-    Stream<RATES, CONS> acc;
+    Stream<RATES, CONS, Geo::PTS> acc;
+    if (Geo::PTS) {
+      acc.pv = pY + tid;
+      acc.ps = NTHREADS;
+    }
     acc.init(fld);
 
     // Bulk-copy staging: thread 0 issues one tensor copy of the halo box per
