@@ -70,9 +70,10 @@ def parse():
                     help="after timing, evolve this many more steps and record the constraint norms")
     ap.add_argument("--track-every", type=int, default=10)
     ap.add_argument("--blocks", type=int, default=0, help="amr3/amr4: block count instead of 600/2000 (small cases)")
-    ap.add_argument("--ozaki-k", type=int, default=0,
+    ap.add_argument("--ozaki-k", default="0",
                     help="ozaki192: one digit count instead of k = 5..8; amr3/amr4: evolve through the "
-                         "Ozaki INT8 derivative path with this many digit planes (0 = float64 stencils)")
+                         "Ozaki INT8 derivative path with this many digit planes (0 = float64 stencils, "
+                         "auto = the smallest k whose rate stays within 1e-10 of float64 on this block list)")
     ap.add_argument("--ozaki-n", type=int, default=192, help="ozaki192: interior points per axis")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -396,7 +397,8 @@ def bench_b200(args):
     # the same state (outside the timed region)
     ozaki = m4 = None
     if not args.no_ozaki and not msrk:
-        ozaki = ozaki_leg(torch, dev, U0, grid, dt, args.ozaki_k or 6, max(args.warmup, 3))
+        k_leg = int(args.ozaki_k) if args.ozaki_k.isdigit() and int(args.ozaki_k) > 0 else 6
+        ozaki = ozaki_leg(torch, dev, U0, grid, dt, k_leg, max(args.warmup, 3))
     if not args.no_m4 and not msrk:
         m4 = m4_leg(torch, dev, U0, grid, dt, max(args.warmup, 3))
 
@@ -631,7 +633,16 @@ def bench_amr(args):
     blocks, punct, dt = amr.workload(index, count=args.blocks or None)
     pool = amr.BlockPool(blocks)
     U0 = torch.from_numpy(pool.initial_state(punct, seed=0)).to(dev)
-    oz_k = int(args.ozaki_k)
+    oz_k = int(args.ozaki_k) if args.ozaki_k.isdigit() else 0
+    k_choice = None
+    if args.ozaki_k == "auto":
+        from bssn3d_b200.ozaki import choose_k
+        chosen, k_errs = choose_k(pool, U0, dt, ghosts=args.ghosts, device=dev)
+        oz_k = chosen or 8
+        k_choice = {"chosen": chosen, "worst_field_err_by_k": {str(k): v for k, v in k_errs.items()},
+                    "bar": 1e-10, "what": "RHS (first-stage accumulator, no KO) vs the float64 block path, per field "
+                                                 "max|diff| / max|fp64| over the interiors"}
+        torch.cuda.empty_cache()
     t_plan = time.time()
     if oz_k:
         from bssn3d_b200.ozaki import BatchedOzakiEvolution
@@ -699,6 +710,26 @@ def bench_amr(args):
         per_stage = fills + 1 + sum(1 for f in range(24) for a in range(3)
                                     if evo.ntiles_kind[_oz_kind(f, a)] > 0) + 33
     del graph
+    # the comparison point: the same step with one stage launch per block
+    per_block = None
+    if not oz_k:
+        gpb, _, _ = evo.capture_per_block(U0, evo.scalars(0.0, dt))
+        for _ in range(max(args.warmup, 1)):
+            gpb.replay()
+        torch.cuda.synchronize(dev)
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.steps):
+            gpb.replay()
+        p1.record(stream)
+        p1.synchronize()
+        pms = p0.elapsed_time(p1) / args.steps
+        per_block = {"ms_per_step": pms, "value": interior * 4 / (pms * 1e-3) / 1e6, "unit": UNIT,
+                     "stage_launches_per_step": 4 * len(evo.active),
+                     "persistent_over_per_block": pms / (ms / args.steps),
+                     "what": "the same captured step with one batched-stage launch per block (one-entry "
+                             "block tables, same tile variant and fills) instead of one persistent launch"}
+        del gpb
     tracked = tracked_fp64 = drift = None
     if args.track > 0:
         # a fresh run from t = 0 on its own captured step
@@ -736,14 +767,17 @@ def bench_amr(args):
                                f"(amr.workload({index})), interiors 16^3/24^3/32^3 +3 ghosts",
                    "ghosts": args.ghosts, "interior_points": interior, "points": pool.points,
                    "state_bytes": int(pool.size * 8), "variant": None if oz_k else variant,
-                   "autotune_ms": {str(k): v for k, v in tune.items()},
+                   "block_order": None if oz_k else evo.order,
+                   "autotune_ms": {f"{k[0]},{k[1]}": v for k, v in tune.items()},
+                   "autotune": "tile variant x block order, one captured step each; fastest kept",
                    "plan_s": round(t_plan, 2), "parallelism": f"replicas x{world}"},
         "clocks": clk, "gpu_launches": (4 * per_stage + 1) * args.steps, "finite": finite,
         "ghost_points": ghost_counts, "breakdown": breakdown,
         "constraints": tracked, "roofline": None, "e2e": None, "cpu_baseline": None,
+        "per_block_launches": per_block,
     }
     if oz_k:
-        line["ozaki"] = {"k": oz_k, "constraints_fp64": tracked_fp64,
+        line["ozaki"] = {"k": oz_k, "k_choice": k_choice, "constraints_fp64": tracked_fp64,
                          "state_vs_fp64_after_track": drift}
     if world > 1:
         import torch.distributed as dist
@@ -788,7 +822,8 @@ def bench_ozaki(args):
     den = ref.reshape(24, -1).abs().amax(dim=1)
     sweep = {}
     chosen = None
-    for k in ((args.ozaki_k,) if args.ozaki_k else (5, 6, 7, 8)):
+    one_k = int(args.ozaki_k) if args.ozaki_k.isdigit() else 0
+    for k in ((one_k,) if one_k else (5, 6, 7, 8)):
         oz = OzakiDerivatives(U.shape[1:], k, device=dev)
         ms = timed(lambda: oz.rhs(U, S), args.steps)
         out = oz.rhs(U, S)

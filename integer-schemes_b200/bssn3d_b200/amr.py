@@ -198,9 +198,11 @@ class BatchedEvolution:
     :func:`autotune` to choose it for a given block list.
     """
 
+    ORDERS = ("pool", "size")
+
     def __init__(self, pool: BlockPool, params=None, ko_sigma: float = 0.1, ko_order: int = 6,
                  variant: int = 0, device="cuda", ghosts: str = "evolve", restrict: bool = False,
-                 plan=None, active=None):
+                 plan=None, active=None, order: str = "pool"):
         import torch
         from .state import PhysicsParams
         from . import _lib
@@ -226,13 +228,28 @@ class BatchedEvolution:
             from .ghosts import DevicePlan, GhostPlan
             self.plan = plan if plan is not None else GhostPlan(pool, restrict=restrict)
             self.dplan = DevicePlan(self.plan, self.device)
-        self.set_variant(variant)
+        self.order = "pool"
+        self.set_variant(variant, order)
         self._bufs = None
 
-    def set_variant(self, variant: int) -> None:
+    def launch_order(self, order: str):
+        """The active blocks in the order their tiles are laid out for the
+        persistent launch (the block-to-CTA mapping: CTA c takes global tiles
+        c, c + grid, ...): ``"pool"`` keeps pool order; ``"size"`` puts the
+        largest blocks first, so the last tiles handed out are small ones."""
+        if order == "pool":
+            return list(self.active)
+        if order == "size":
+            return sorted(self.active, key=lambda i: (-self.pool.blocks[i].points, i))
+        raise ValueError(f"order must be one of {self.ORDERS}, not {order!r}")
+
+    def set_variant(self, variant: int, order: str = None) -> None:
+        """Tile variant and block order of the batched stage launches."""
         import torch
         lib = self._lib.load()
-        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange", active=self.active)
+        order = self.order if order is None else order
+        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange",
+                                         active=self.launch_order(order))
         ntiles = lib.bssn_b200_batch_plan(ctypes.addressof(table), len(self.active), int(variant))
         if ntiles < 0:
             self._lib.check(self._lib.EINVAL)
@@ -240,6 +257,7 @@ class BatchedEvolution:
         self.table_dev = torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(self.device)
         self.ntiles = int(ntiles)
         self.variant = int(variant)
+        self.order = order
 
     def scalars(self, t: float, dt: float):
         from .fused_rhs import device_scalars, scalars
@@ -347,6 +365,69 @@ class BatchedEvolution:
         return U_g
 
     # -- the comparison point: one launch per block per stage ----------------
+    def per_block_tables(self):
+        """One single-block table per active block (same kernel, same tile
+        variant, same covered points as the persistent launch), in one device
+        buffer: (buffer, byte offsets, tile counts)."""
+        import torch
+        lib = self._lib.load()
+        table, _ = self.pool.descriptors(self.pool.tile, core=self.ghosts == "exchange", active=self.active)
+        raw, offs, ntiles = bytearray(), [], []
+        for j in range(len(self.active)):
+            one = BlockDesc.from_buffer_copy(table[j])
+            n = lib.bssn_b200_batch_plan(ctypes.addressof(one), 1, self.variant)
+            if n < 0:
+                self._lib.check(self._lib.EINVAL)
+            offs.append(len(raw))
+            ntiles.append(int(n))
+            raw += bytes(memoryview(one).cast("B"))
+            raw += bytes((-len(raw)) % 16)
+        return torch.frombuffer(raw, dtype=torch.uint8).to(self.device), offs, ntiles
+
+    def per_block_launch_step_inplace(self, U, S, tables=None):
+        """The RK4 step of :meth:`step_inplace` with one batched-stage launch
+        per block (a one-entry block table each) instead of one persistent
+        launch over all blocks: the same kernel, tiles and results, so the
+        difference in time is the launch structure alone."""
+        lib = self._lib.load()
+        buf, offs, ntiles = tables if tables is not None else self.per_block_tables()
+        b = self.buffers(U)
+        p = self.params
+        for stage, (y, ynext) in enumerate([(U, b["Ya"]), (b["Ya"], b["Yb"]), (b["Yb"], b["Ya"]),
+                                            (b["Ya"], U)]):
+            self.fill(y)
+            for o, nt in zip(offs, ntiles):
+                rc = lib.bssn_b200_batch_rk4_stage(self._stream(), stage, U.data_ptr(), y.data_ptr(),
+                                                   b["ACC"].data_ptr(), ynext.data_ptr(), S.data_ptr(),
+                                                   self.ko_sigma, self.ko_order, p.chi_floor, p.alpha_floor,
+                                                   buf.data_ptr() + o, 1, nt, self.variant)
+                self._lib.check(rc)
+        if self.plan is not None and self.plan.restrict_lists:
+            self.restrict(U)
+
+    def capture_per_block(self, U, S):
+        """:meth:`capture` for the one-launch-per-block step."""
+        import torch
+        tables = self.per_block_tables()
+        U_g, S_g = U.clone(), S.clone()
+        self.buffers(U_g)
+        if self.ghosts == "exchange":
+            self.seed_buffers(U_g)
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            pu, ps = U_g.clone(), S_g.clone()
+            self.per_block_launch_step_inplace(pu, ps, tables)
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        del pu, ps
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.per_block_launch_step_inplace(U_g, S_g, tables)
+            self.advance_time(S_g)
+        g.static_tensors = (U_g, S_g, self.buffers(U_g), tables[0], self.dplan)
+        return g, U_g, S_g
+
     def per_block_step_inplace(self, U, S_blocks):
         """The same RK4 step with one uniform-kernel launch per block per
         stage (``S_blocks[i]`` carries block i's spacing); blocks evolve on
@@ -409,27 +490,34 @@ class BatchedEvolution:
                 for blk in self.pool.blocks]
 
 
-def autotune(evo: BatchedEvolution, U, dt: float, variants=None, reps: int = 3):
-    """Time one captured RK4 step per tile variant on this block list and keep
-    the fastest. Returns {variant: ms} and leaves ``evo`` on the winner."""
+def autotune(evo: BatchedEvolution, U, dt: float, variants=None, orders=None, reps: int = 3):
+    """Time one captured RK4 step for every (tile variant, block order) on
+    this block list and keep the fastest. The tile shape and the block-to-CTA
+    mapping are the kernel's launch knobs; its register cap is fixed at one
+    255-register CTA per SM (a two-CTA, 128-register build of the same kernel
+    spills ~3.7 KB per thread and measured slower on B200). Returns
+    {(variant, order): ms} and leaves ``evo`` on the winner."""
     import torch
     from . import _lib
     variants = range(_lib.NVARIANTS) if variants is None else variants
+    orders = BatchedEvolution.ORDERS if orders is None else orders
     times = {}
     for v in variants:
-        evo.set_variant(v)
-        g, U_g, _ = evo.capture(U, evo.scalars(0.0, dt))
-        g.replay()
-        torch.cuda.synchronize(evo.device)
-        best = float("inf")
-        for _ in range(reps):
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record()
+        for order in orders:
+            evo.set_variant(v, order)
+            g, U_g, _ = evo.capture(U, evo.scalars(0.0, dt))
             g.replay()
-            b.record()
-            b.synchronize()
-            best = min(best, a.elapsed_time(b))
-        times[v] = best
-        del g, U_g
-    evo.set_variant(min(times, key=times.get))
+            torch.cuda.synchronize(evo.device)
+            best = float("inf")
+            for _ in range(reps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
+                g.replay()
+                b.record()
+                b.synchronize()
+                best = min(best, a.elapsed_time(b))
+            times[(v, order)] = best
+            del g, U_g
+    v, order = min(times, key=times.get)
+    evo.set_variant(v, order)
     return times

@@ -80,10 +80,29 @@ def test_batched_ko8_ghost4():
         assert O.normwise_rel_grouped(pool.gather(new, i), ref).max() < 1e-12
 
 
-def test_autotune_picks_a_variant():
+def test_autotune_picks_a_variant_and_block_order():
     from bssn3d_b200 import amr
     pool, U, _ = _small_pool(count=8, seed=1)
     evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6)
     times = amr.autotune(evo, torch.from_numpy(U).cuda(), 0.01, reps=2)
-    assert sorted(times) == [0, 1, 2, 3]
-    assert evo.variant == min(times, key=times.get)
+    assert sorted(times) == [(v, o) for v in range(4) for o in sorted(amr.BatchedEvolution.ORDERS)]
+    assert (evo.variant, evo.order) == min(times, key=times.get)
+
+
+@pytest.mark.parametrize("ghosts", ["evolve", "exchange"])
+def test_block_order_and_one_launch_per_block_give_the_same_bytes(ghosts):
+    """The block-to-CTA mapping and the launch structure change only which CTA
+    computes a tile, never its arithmetic: every form gives the same bytes."""
+    from bssn3d_b200 import amr
+    pool, U, _ = _small_pool(count=6, seed=11)
+    dt = 0.25 * min(b.h for b in pool.blocks)
+    Ud = torch.from_numpy(U).cuda()
+    evo = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, variant=2, ghosts=ghosts)
+    base = evo.evolve(Ud, dt, 2).cpu().numpy()
+    evo.set_variant(2, "size")
+    assert evo.launch_order("size") != evo.launch_order("pool")
+    np.testing.assert_array_equal(evo.evolve(Ud, dt, 2).cpu().numpy(), base)
+    g, U_g, _ = evo.capture_per_block(Ud, evo.scalars(0.0, dt))
+    for _ in range(2):
+        g.replay()
+    np.testing.assert_array_equal(U_g.cpu().numpy(), base)

@@ -142,3 +142,16 @@ def test_graph_replay_equals_eager_steps():
     torch.cuda.synchronize()
     oz.check()
     assert torch.equal(got, eager)
+
+
+def test_choose_k_takes_the_smallest_k_within_the_bar():
+    """The autotuner's digit-count knob: errors of the block-list RHS fall
+    with k, and the chosen k is the first whose worst field meets the bar."""
+    from bssn3d_b200.ozaki import choose_k
+    pool, punct = _pool(count=6, seed=3)
+    U = torch.from_numpy(pool.initial_state(punct, seed=2)).cuda()
+    dt = 0.25 * min(b.h for b in pool.blocks)
+    k, errs = choose_k(pool, U, dt, ks=(4, 5, 6, 7, 8), bar=1e-10)
+    assert errs[4] > errs[5] > errs[6] > errs[7] > errs[8]
+    assert k == min(q for q in errs if errs[q] <= 1e-10)
+    assert errs[8] < 1e-12
