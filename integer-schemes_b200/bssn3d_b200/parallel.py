@@ -7,7 +7,9 @@ units and the ranks exchange nothing while they step. With ghost exchange
 other ranks: every rank computes the same global fill plan, keeps mirror
 copies of the remote blocks its own ghosts read, and before each level's
 fill receives those blocks from their owners (point-to-point, NCCL between
-GPUs); the constraint norms take one all-reduce. Ranges are cut so that
+GPUs) — only the points its fill boxes read, gathered into one buffer per
+peer and level (whole mirrored blocks are the fallback); the constraint
+norms take one all-reduce. Ranges are cut so that
 every rank holds about the same cost (the fused kernel's work is
 proportional to the padded volume).
 """
@@ -51,6 +53,37 @@ def partition(blocks: Sequence, world: int) -> List[List[int]]:
 
 def local_blocks(blocks: Sequence, rank: int, world: int):
     return [blocks[i] for i in partition(blocks, world)[rank]]
+
+
+def read_box(op):
+    """The box of source-block points a fill op reads, half-open per axis
+    ((lo, hi) x 3), clamped to the source array: the shifted destination box
+    for a same-level copy; for a prolongation, the source nodes of every
+    refined index g = d + shift (node g/2 for even g, the six nodes
+    (g-1)/2 - 2 ... (g-1)/2 + 3 for odd g). Restriction ops are not read
+    across ranks."""
+    from .ghosts import COPY, PROLONG
+    box = []
+    for a in range(3):
+        s = op.src_s[a]
+        gmin, gmax = op.lo[a] + op.shift[a], op.hi[a] - 1 + op.shift[a]
+        if op.kind == COPY:
+            lo, hi = gmin, gmax + 1
+        elif op.kind == PROLONG:
+            lo, hi = (gmin - 1) // 2 - 2, (gmax - 1) // 2 + 3 + 1
+        else:
+            raise ValueError("restriction ops are not exchanged across ranks")
+        box.append((max(lo, 0), min(hi, s)))
+    return box
+
+
+def box_points(box, shape) -> "np.ndarray":
+    """Flat in-block indices (C order) of the points of ``box``."""
+    import numpy as np
+    (x0, x1), (y0, y1), (z0, z1) = box
+    sy, sz = shape[1], shape[2]
+    x, y, z = np.meshgrid(np.arange(x0, x1), np.arange(y0, y1), np.arange(z0, z1), indexing="ij")
+    return ((x * sy + y) * sz + z).reshape(-1).astype(np.int64)
 
 
 class RankLayout:
@@ -112,6 +145,90 @@ class RankLayout:
                      for lvl in self.levels}
         self.recv = {lvl: sorted(v, key=lambda t: (t[1], t[0])) for lvl, v in self.recv.items()}
         self.g2l = g2l
+        # Packed halos: the points of a remote block that a rank's fill reads
+        # at a level (the union of its ops' read boxes), so that only those
+        # cross between ranks instead of whole block arrays.
+        import numpy as np
+        reads = {r: {} for r in range(world)}   # r -> {(lvl, j): point indices}
+        for r in range(world):
+            for lvl, keep in per_rank_ops[r]:
+                for op in keep:
+                    j = off2idx[op.src_off]
+                    if owner[j] == r:
+                        continue
+                    pts = box_points(read_box(op), blocks[j].shape)
+                    key = (lvl, j)
+                    reads[r][key] = pts if key not in reads[r] else np.union1d(reads[r][key], pts)
+        self._reads = reads
+        self._packed = {}
+
+    def _pack_index(self, pairs, points_of):
+        """Flat pool indices (24 fields x points, block by block in the given
+        order) of the packed points of ``pairs`` [(peer, global block)]."""
+        import numpy as np
+        parts = []
+        for _, j in pairs:
+            pts = points_of(j)
+            i = self.g2l[j]
+            o, n = int(self.pool.offsets[i]), self.pool.blocks[i].points
+            parts.append((o + np.arange(24, dtype=np.int64)[:, None] * n + pts[None, :]).reshape(-1))
+        return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
+
+    def packed_plan(self, device):
+        """Per level and peer, the device index lists of the packed exchange:
+        {level: ([(peer, send index)], [(peer, recv index)])}, messages in
+        global block order (both sides build them from the same global plan)."""
+        import torch
+        key = str(device)
+        if key in self._packed:
+            return self._packed[key]
+        plan = {}
+        for lvl in self.levels:
+            sends, recvs = [], []
+            for q in range(self.world):
+                sp = [(q2, j) for q2, j in self.send.get(lvl, []) if q2 == q]
+                if sp:
+                    idx = self._pack_index(sp, lambda j, q=q: self._reads[q][(lvl, j)])
+                    sends.append((q, torch.from_numpy(idx).to(device)))
+                rp = [(p, j) for p, j in self.recv.get(lvl, []) if p == q]
+                if rp:
+                    idx = self._pack_index(rp, lambda j: self._reads[self.rank][(lvl, j)])
+                    recvs.append((q, torch.from_numpy(idx).to(device)))
+            plan[lvl] = (sends, recvs)
+        self._packed[key] = plan
+        return plan
+
+    def exchange_bytes(self, packed: bool = True) -> int:
+        """Bytes this rank sends per fill (all levels), packed or whole blocks."""
+        total = 0
+        for lvl in self.levels:
+            for q, j in self.send.get(lvl, []):
+                total += 8 * 24 * (len(self._reads[q][(lvl, j)]) if packed else self.pool.blocks[self.g2l[j]].points)
+        return total
+
+    def exchange_packed(self, pool_tensor, level: int, group=None) -> None:
+        """:meth:`exchange` moving only the points the receivers' fill boxes
+        read: one gathered buffer per peer and level each way, scattered into
+        the mirrors on arrival. Mirror points outside the read boxes are not
+        kept up to date (no fill box reads them)."""
+        import torch
+        import torch.distributed as dist
+        if self.world == 1:
+            return
+        sends, recvs = self.packed_plan(pool_tensor.device)[level]
+        flat = pool_tensor.view(-1)
+        ops, bufs = [], []
+        for q, idx in sends:
+            ops.append(dist.P2POp(dist.isend, flat[idx], q, group=group))
+        for p, idx in recvs:
+            buf = torch.empty(idx.numel(), dtype=pool_tensor.dtype, device=pool_tensor.device)
+            bufs.append((idx, buf))
+            ops.append(dist.P2POp(dist.irecv, buf, p, group=group))
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+        for idx, buf in bufs:
+            flat[idx] = buf
 
     def block_view(self, pool_tensor, g: int):
         """The flat view of global block ``g`` in this rank's pool tensor."""
@@ -137,17 +254,19 @@ class RankLayout:
 
 class DistributedBatchedEvolution:
     """RK4 over a block list split across ranks, ghosts exchanged each stage:
-    per stage, per level from coarse to fine, the mirrors this rank's fill
-    reads are received from their owners, then the level's fill boxes run
+    per stage, per level from coarse to fine, the points of remote blocks this
+    rank's fill reads are received from their owners (packed; whole blocks
+    with ``packed=False``), then the level's fill boxes run
     (``bssn_b200_fill``), then one batched stage launch evolves this rank's
     own blocks. Eager (not graph-captured: the point-to-point transfers sit
     between the launches). ``world == 1`` is the single-GPU exchange path."""
 
     def __init__(self, blocks: Sequence, punctures=None, world: int = 1, rank: int = 0, ko_sigma: float = 0.1,
-                 ko_order: int = 6, variant: int = 0, device="cuda", group=None):
+                 ko_order: int = 6, variant: int = 0, device="cuda", group=None, packed: bool = True):
         from .amr import BatchedEvolution
         self.layout = RankLayout(blocks, world, rank)
         self.group = group
+        self.packed = bool(packed)
         self.evo = BatchedEvolution(self.layout.pool, ko_sigma=ko_sigma, ko_order=ko_order, variant=variant,
                                     device=device, ghosts="exchange", plan=self.layout,
                                     active=self.layout.owned)
@@ -155,7 +274,10 @@ class DistributedBatchedEvolution:
     def fill(self, Y) -> None:
         stream = self.evo._stream()
         for lvl in self.layout.levels:
-            self.layout.exchange(Y, lvl, self.group)
+            if self.packed:
+                self.layout.exchange_packed(Y, lvl, self.group)
+            else:
+                self.layout.exchange(Y, lvl, self.group)
             self.evo.dplan.run_level("fill", lvl, Y, stream)
 
     def step_inplace(self, U, S) -> None:

@@ -74,7 +74,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _worker(rank, world, port, seed, out):
+def _worker(rank, world, port, seed, out, packed=False):
     import torch.distributed as dist
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
@@ -92,7 +92,10 @@ def _worker(rank, world, port, seed, out):
             lay.block_view(local, g).copy_(torch.from_numpy(state[o:o + 24 * blocks[g].points]))
         arr = local.numpy()
         for lvl in lay.levels:
-            lay.exchange(local, lvl)
+            if packed:
+                lay.exchange_packed(local, lvl)
+            else:
+                lay.exchange(local, lvl)
             _run_level(lay.pool, lay.fill_lists, lvl, arr)
         want = A.fill(state, A.geometry_of(gpool))
         ok = True
@@ -105,16 +108,43 @@ def _worker(rank, world, port, seed, out):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_fill_like_one_process(world):
+@pytest.mark.parametrize("world,packed", [(2, False), (3, False), (2, True), (3, True)])
+def test_gloo_ranks_fill_like_one_process(world, packed):
     import torch.multiprocessing as mp
     ctx = mp.get_context("spawn")
     out = ctx.Manager().dict()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, world, port, 3, out)) for r in range(world)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, 3, out, packed)) for r in range(world)]
     for p in procs:
         p.start()
     for p in procs:
         p.join(timeout=300)
         assert p.exitcode == 0
     assert dict(out) == {r: 1 for r in range(world)}
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_packed_exchange_moves_only_the_read_points(world):
+    """The packed halos are a subset of the whole mirrored blocks, cover
+    every point a rank's fill boxes read, and move fewer bytes."""
+    from bssn3d_b200 import amr, ghosts
+    from bssn3d_b200.parallel import RankLayout, read_box
+    blocks = _blocks()
+    gplan = ghosts.GhostPlan(amr.BlockPool(blocks))
+    lays = [RankLayout(blocks, world, r, plan=gplan) for r in range(world)]
+    packed = sum(L.exchange_bytes(True) for L in lays)
+    whole = sum(L.exchange_bytes(False) for L in lays)
+    assert 0 < packed < whole
+    for L in lays:
+        for lvl, ops in L.fill_lists:
+            for op in ops:
+                g = L.index[[int(o) for o in L.pool.offsets].index(op.src_off)]
+                if g in L.parts[L.rank]:
+                    continue
+                pts = set(L._reads[L.rank][(lvl, g)].tolist())
+                (x0, x1), (y0, y1), (z0, z1) = read_box(op)
+                sy, sz = op.src_s[1], op.src_s[2]
+                for x in (x0, x1 - 1):
+                    for y in (y0, y1 - 1):
+                        for z in (z0, z1 - 1):
+                            assert (x * sy + y) * sz + z in pts
