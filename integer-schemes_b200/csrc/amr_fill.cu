@@ -7,11 +7,13 @@
 //
 // A fill is a host-planned list of boxes (bssn_b200_fill_op), copies and
 // injections first, prolongations after (fewer warps mix the two paths). One
-// launch executes one list: every thread takes one destination point
-// (flattened over the boxes by a prefix of box volumes, its box found by
-// binary search) and moves all 24 fields. The work is a gather of a small
-// part of the pool and bound by memory latency: the copy path issues its 24
-// loads before its stores, and the grid holds four CTAs per SM.
+// launch executes one list: a thread takes one copied point and moves all 24
+// fields, or one (prolongated point, field) pair (points flattened over the
+// boxes by a prefix of box volumes, the box found by binary search). The work
+// is a gather of a small part of the pool and bound by memory latency: the
+// copy path issues its 24 loads before its stores, prolongations run one
+// field per thread and a warp's points share their parity class, and the grid
+// holds four CTAs per SM.
 //
 // Prolongation refines the source block x, then y, then z. A point odd on an
 // axis sums its 6 taps in offset order starting from 0 (the reference's
@@ -109,7 +111,7 @@ __device__ __forceinline__ bool decode_by_parity(const bssn_b200_fill_op& op, lo
 }
 
 __device__ __forceinline__ void prolong_point(double* __restrict__ pool, const bssn_b200_fill_op& op, long long p,
-                                              const double* __restrict__ w) {
+                                              const double* __restrict__ w, int f) {
   int d0, d1, d2;
   if (!decode_by_parity(op, p, d0, d1, d2)) return;
   const int ss0 = op.src_s[0], ss1 = op.src_s[1], ss2 = op.src_s[2];
@@ -123,7 +125,7 @@ __device__ __forceinline__ void prolong_point(double* __restrict__ pool, const b
   const int k0 = g0 >> 1, k1 = g1 >> 1, k2 = g2 >> 1;  // arithmetic shift: floor(g / 2)
   const int ny = o1 ? 6 : 1, nz = o2 ? 6 : 1;
   const long long sxs = (long long)ss1 * ss2;
-  for (int f = 0; f < NFIELD; ++f) {
+  {
     const double* P = src + f * ns;
     double vz = 0.0;
     for (int c = 0; c < nz; ++c) {
@@ -148,25 +150,49 @@ __device__ __forceinline__ void prolong_point(double* __restrict__ pool, const b
   }
 }
 
-// Every thread takes points p by a grid stride and finds its box by binary
-// search over the boxes' point prefix.
+// Work items: every copied or injected point (24 fields each), then every
+// (prolongated point, field) pair — a prolongation sums up to 216 taps per
+// field, so its fields go to separate threads; 32 consecutive items of a warp
+// are 32 consecutive points of one field. Every thread takes items by a grid
+// stride and finds its box by binary search over the boxes' point prefix.
 __global__ void __launch_bounds__(NTHREADS, MIN_CTAS) fill_kernel(double* __restrict__ pool,
                                                                   const bssn_b200_fill_op* __restrict__ ops,
                                                                   int nops, long long npoints, const Wmid W) {
   __shared__ double sw[6];  // midpoint weights (indexed by tap)
+  __shared__ long long ncopy_s;  // points before the first prolongation box
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int j = 0; j < 6; ++j) sw[j] = W.w[j];
+    int lo = 0, hi = nops;  // first prolongation op (the list has them last)
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ops[mid].kind == BSSN_B200_FILL_PROLONG) hi = mid; else lo = mid + 1;
+    }
+    ncopy_s = lo < nops ? ops[lo].point0 : npoints;
   }
   __syncthreads();
+  const long long ncopy = ncopy_s;
+  // whole 32-point chunks of prolongation items (the last one's tail skips)
+  const long long items = ncopy + (npoints - ncopy + 31) / 32 * 32 * NFIELD;
   const long long stride = (long long)gridDim.x * NTHREADS;
-  for (long long p = (long long)blockIdx.x * NTHREADS + threadIdx.x; p < npoints; p += stride) {
+  for (long long it = (long long)blockIdx.x * NTHREADS + threadIdx.x; it < items; it += stride) {
+    long long p;
+    int f = 0;
+    if (it < ncopy) {
+      p = it;
+    } else {
+      const long long q = it - ncopy;
+      const long long r = q % (32 * NFIELD);
+      f = (int)(r >> 5);
+      p = ncopy + (q / (32 * NFIELD)) * 32 + (r & 31);
+      if (p >= npoints) continue;
+    }
     int lo = 0, hi = nops - 1;  // last box with point0 <= p
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
       if (ops[mid].point0 <= p) lo = mid; else hi = mid - 1;
     }
-    if (ops[lo].kind == BSSN_B200_FILL_PROLONG) prolong_point(pool, ops[lo], p, sw);
+    if (ops[lo].kind == BSSN_B200_FILL_PROLONG) prolong_point(pool, ops[lo], p, sw, f);
     else copy_point(pool, ops[lo], p);
   }
 }
@@ -249,7 +275,7 @@ int bssn_b200_fill(void* stream, double* pool, const bssn_b200_fill_op* ops, int
   int sms = 0;
   int rc = bssn_host::device_sms(&sms);
   if (rc) return rc;
-  const long long want = (npoints + amr::NTHREADS - 1) / amr::NTHREADS;
+  const long long want = (npoints * amr::NFIELD + amr::NTHREADS - 1) / amr::NTHREADS;
   const long long cap = 4LL * amr::MIN_CTAS * sms;  // four waves of resident CTAs
   amr::fill_kernel<<<(int)(want < cap ? want : cap), amr::NTHREADS, 0, static_cast<cudaStream_t>(stream)>>>(
       pool, ops, nops, npoints, W);
