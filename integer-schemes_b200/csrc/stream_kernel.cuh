@@ -391,6 +391,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
     __syncthreads();
   }
   int cur_block = -1;
+  bool prefetched = false;  // the tile's first field was staged during the previous tile
 
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
     // ---- tile geometry: the single grid, or the block that owns this tile ----
@@ -499,10 +500,11 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
     // after the barrier that frees their buffer
     if (TMA) {
       tma_issue(stream_field(0), 0);
-    } else {
+    } else if (!prefetched) {
       stage_tile<R, T, ZS>(bufp(0), Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
       cp_async_commit();
     }
+    prefetched = false;
     Unroll<0, NFIELD>::run([&](auto ic) {
       constexpr int idx = decltype(ic)::value;
       constexpr int f = stream_field(idx);
@@ -530,6 +532,16 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
           stage_tile<R, T, ZS>(bufp((idx + 1) % NB), Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
                                Sx, Sy, Sz, tid);
           cp_async_commit();
+        } else if (!batched && tile + (int)gridDim.x < ntiles) {
+          // single grid: the next tile's first field into the buffer that
+          // field idx - 1 just freed, so its copies overlap this tile's last
+          // field and epilogue
+          const int nt = tile + (int)gridDim.x;
+          const int nz_ = nt % ntz, ny_ = (nt / ntz) % nty, nx_ = nt / (ntz * nty);
+          stage_tile<R, T, ZS>(bufp((idx + 1) % NB), args.F + (long long)stream_field(0) * n, (long long)nx_ * TX,
+                               (long long)ny_ * TY, (long long)nz_ * TZ, Sx, Sy, Sz, tid);
+          cp_async_commit();
+          prefetched = true;
         }
       }
 
