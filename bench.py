@@ -172,23 +172,34 @@ def reference_step_sample(n_interior: int, planes: int = 8):
 
 
 def run_cpu_reference(U, S, steps, warmup, threads):
-    """RK4 steps of evolve.py:125-137 with the reference's compiled algebra."""
+    """RK4 steps of evolve.py:125-137 with the reference's compiled algebra;
+    the stage combinations run as multithreaded torch CPU operations on the
+    same host threads as the OpenMP algebra."""
+    import torch
     from oracle import oracle as O
     os.environ["OMP_NUM_THREADS"] = str(threads)
-    dt = S[2]
+    torch.set_num_threads(threads)
+    dt = float(S[2])
     g = (S[13], S[14], S[15])
+    T = torch.from_numpy
 
     def rate(Y, tt):
         S2 = S.copy()
         S2[6] = tt
-        return O.ref_rhs(Y, S2, nthreads=threads) + O.ko(Y, *g, 0.1, 6)
+        r = T(O.ref_rhs(Y, S2, nthreads=threads))
+        r.add_(T(O.ko(Y, *g, 0.1, 6)))
+        return r
+
+    def axpy(u, a, k):
+        return torch.add(T(u), k, alpha=a).numpy()
 
     def step(U, t):
         k1 = rate(U, t)
-        k2 = rate(U + 0.5 * dt * k1, t + 0.5 * dt)
-        k3 = rate(U + 0.5 * dt * k2, t + 0.5 * dt)
-        k4 = rate(U + dt * k3, t + dt)
-        return O.enforce(U + (dt / 6.0) * (k1 + 2 * k2 + 2 * k3 + k4))
+        k2 = rate(axpy(U, 0.5 * dt, k1), t + 0.5 * dt)
+        k3 = rate(axpy(U, 0.5 * dt, k2), t + 0.5 * dt)
+        k4 = rate(axpy(U, dt, k3), t + dt)
+        acc = k1.add_(k2, alpha=2.0).add_(k3, alpha=2.0).add_(k4)
+        return O.enforce(axpy(U, dt / 6.0, acc))
 
     t = 0.0
     for _ in range(warmup):
