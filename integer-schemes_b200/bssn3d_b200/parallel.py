@@ -8,8 +8,10 @@ other ranks: every rank computes the same global fill plan, keeps mirror
 copies of the remote blocks its own ghosts read, and before each level's
 fill receives those blocks from their owners (point-to-point, NCCL between
 GPUs) — only the points its fill boxes read, gathered into one buffer per
-peer and level (whole mirrored blocks are the fallback); the constraint
-norms take one all-reduce. Ranges are cut so that
+peer and level (whole mirrored blocks are the fallback); the optional
+restriction after a step receives the remote fine points it injects the same
+way, finest level first; the constraint norms take one all-reduce. Ranges
+are cut so that
 every rank holds about the same cost (the fused kernel's work is
 proportional to the padded volume).
 """
@@ -60,9 +62,9 @@ def read_box(op):
     ((lo, hi) x 3), clamped to the source array: the shifted destination box
     for a same-level copy; for a prolongation, the source nodes of every
     refined index g = d + shift (node g/2 for even g, the six nodes
-    (g-1)/2 - 2 ... (g-1)/2 + 3 for odd g). Restriction ops are not read
-    across ranks."""
-    from .ghosts import COPY, PROLONG
+    (g-1)/2 - 2 ... (g-1)/2 + 3 for odd g); for an injection the box spanned
+    by 2 d + shift (it reads every other point of it, see :func:`read_points`)."""
+    from .ghosts import COPY, PROLONG, RESTRICT
     box = []
     for a in range(3):
         s = op.src_s[a]
@@ -71,10 +73,24 @@ def read_box(op):
             lo, hi = gmin, gmax + 1
         elif op.kind == PROLONG:
             lo, hi = (gmin - 1) // 2 - 2, (gmax - 1) // 2 + 3 + 1
+        elif op.kind == RESTRICT:
+            lo, hi = 2 * op.lo[a] + op.shift[a], 2 * (op.hi[a] - 1) + op.shift[a] + 1
         else:
-            raise ValueError("restriction ops are not exchanged across ranks")
+            raise ValueError(f"unknown fill kind {op.kind}")
         box.append((max(lo, 0), min(hi, s)))
     return box
+
+
+def read_points(op, shape) -> "np.ndarray":
+    """Flat in-block indices of the source points an op reads: its read box,
+    or for an injection (src[2 d + shift]) every other point of it."""
+    import numpy as np
+    from .ghosts import RESTRICT
+    if op.kind != RESTRICT:
+        return box_points(read_box(op), shape)
+    ax = [2 * np.arange(op.lo[a], op.hi[a]) + op.shift[a] for a in range(3)]
+    x, y, z = np.meshgrid(*ax, indexing="ij")
+    return ((x * shape[1] + y) * shape[2] + z).reshape(-1).astype(np.int64)
 
 
 def box_points(box, shape) -> "np.ndarray":
@@ -100,6 +116,7 @@ class RankLayout:
 
     def __init__(self, blocks: Sequence, world: int, rank: int, plan=None):
         import ctypes as _ct
+        import numpy as np
         from .amr import BlockPool
         from .ghosts import FillOp, GhostPlan
         self.world, self.rank = int(world), int(rank)
@@ -110,57 +127,73 @@ class RankLayout:
                 owner[i] = r
         gpool = BlockPool(blocks)
         gplan = plan if plan is not None else GhostPlan(gpool)
-        if gplan.restrict_lists:
-            raise ValueError("restriction across ranks is not provided: build the plan without it")
         off2idx = {int(o): i for i, o in enumerate(gpool.offsets)}
-        # for every rank: the remote sources its own ghost boxes read, per level
-        needs = {r: {} for r in range(world)}
-        per_rank_ops = {r: [] for r in range(world)}
-        for lvl, ops in gplan.fill_lists:
-            for r in range(world):
-                keep = [op for op in ops if owner[off2idx[op.dst_off]] == r]
-                per_rank_ops[r].append((lvl, keep))
-                needs[r][lvl] = sorted({off2idx[op.src_off] for op in keep if owner[off2idx[op.src_off]] != r})
-        mirrors = sorted({j for v in needs[rank].values() for j in v})
+        # Per phase (ghost fill; restriction): the ops each rank runs (those
+        # whose destination it owns), the remote source blocks they read, and
+        # the exact source points read (the union of the ops' read points).
+        phases = {"fill": gplan.fill_lists, "restrict": gplan.restrict_lists}
+        per_rank_ops = {ph: {r: [] for r in range(world)} for ph in phases}
+        needs = {ph: {r: {} for r in range(world)} for ph in phases}
+        reads = {ph: {r: {} for r in range(world)} for ph in phases}
+        for ph, lists in phases.items():
+            for lvl, ops in lists:
+                for r in range(world):
+                    keep = [op for op in ops if owner[off2idx[op.dst_off]] == r]
+                    per_rank_ops[ph][r].append((lvl, keep))
+                    needs[ph][r][lvl] = sorted({off2idx[op.src_off] for op in keep
+                                                if owner[off2idx[op.src_off]] != r})
+                    for op in keep:
+                        j = off2idx[op.src_off]
+                        if owner[j] == r:
+                            continue
+                        pts = read_points(op, blocks[j].shape)
+                        key = (lvl, j)
+                        got = reads[ph][r].get(key)
+                        reads[ph][r][key] = pts if got is None else np.union1d(got, pts)
+        mirrors = sorted({j for ph in phases for v in needs[ph][rank].values() for j in v})
         self.index = sorted(set(self.parts[rank]) | set(mirrors))
         g2l = {g: l for l, g in enumerate(self.index)}
+        self.g2l = g2l
         self.owned = sorted(g2l[g] for g in self.parts[rank])
         self.pool = BlockPool([blocks[i] for i in self.index])
-        self.fill_lists = []
-        for lvl, keep in per_rank_ops[rank]:
-            local = []
-            for op in keep:
-                q = FillOp()
-                _ct.pointer(q)[0] = op
-                q.dst_off = int(self.pool.offsets[g2l[off2idx[op.dst_off]]])
-                q.src_off = int(self.pool.offsets[g2l[off2idx[op.src_off]]])
-                local.append(q)
-            if local:
-                self.fill_lists.append((lvl, local))
-        self.restrict_lists = []
-        self.levels = [lvl for lvl, _ in gplan.fill_lists]
-        self.recv = {lvl: [(owner[j], j) for j in needs[rank][lvl]] for lvl in self.levels}
-        self.send = {lvl: sorted(((q, j) for q in range(world) if q != rank
-                                  for j in needs[q][lvl] if owner[j] == rank), key=lambda t: (t[1], t[0]))
-                     for lvl in self.levels}
-        self.recv = {lvl: sorted(v, key=lambda t: (t[1], t[0])) for lvl, v in self.recv.items()}
-        self.g2l = g2l
-        # Packed halos: the points of a remote block that a rank's fill reads
-        # at a level (the union of its ops' read boxes), so that only those
-        # cross between ranks instead of whole block arrays.
-        import numpy as np
-        reads = {r: {} for r in range(world)}   # r -> {(lvl, j): point indices}
-        for r in range(world):
-            for lvl, keep in per_rank_ops[r]:
+
+        def local_lists(ph):
+            out = []
+            for lvl, keep in per_rank_ops[ph][rank]:
+                local = []
                 for op in keep:
-                    j = off2idx[op.src_off]
-                    if owner[j] == r:
-                        continue
-                    pts = box_points(read_box(op), blocks[j].shape)
-                    key = (lvl, j)
-                    reads[r][key] = pts if key not in reads[r] else np.union1d(reads[r][key], pts)
-        self._reads = reads
+                    q = FillOp()
+                    _ct.pointer(q)[0] = op
+                    q.dst_off = int(self.pool.offsets[g2l[off2idx[op.dst_off]]])
+                    q.src_off = int(self.pool.offsets[g2l[off2idx[op.src_off]]])
+                    local.append(q)
+                if local:
+                    out.append((lvl, local))
+            return out
+
+        def pairs(ph):
+            levels = [lvl for lvl, _ in phases[ph]]
+            recv = {lvl: sorted(((owner[j], j) for j in needs[ph][rank][lvl]), key=lambda t: (t[1], t[0]))
+                    for lvl in levels}
+            send = {lvl: sorted(((q, j) for q in range(world) if q != rank
+                                 for j in needs[ph][q][lvl] if owner[j] == rank), key=lambda t: (t[1], t[0]))
+                    for lvl in levels}
+            return levels, send, recv
+
+        self.fill_lists = local_lists("fill")
+        self.restrict_lists = local_lists("restrict")
+        self.levels, self.send, self.recv = pairs("fill")
+        self.restrict_levels, self.send_restrict, self.recv_restrict = pairs("restrict")
+        self._reads = reads["fill"]
+        self._reads_restrict = reads["restrict"]
         self._packed = {}
+
+    def _phase(self, phase: str):
+        if phase == "fill":
+            return self.levels, self.send, self.recv, self._reads
+        if phase == "restrict":
+            return self.restrict_levels, self.send_restrict, self.recv_restrict, self._reads_restrict
+        raise ValueError(f"phase must be 'fill' or 'restrict', not {phase!r}")
 
     def _pack_index(self, pairs, points_of):
         """Flat pool indices (24 fields x points, block by block in the given
@@ -174,48 +207,52 @@ class RankLayout:
             parts.append((o + np.arange(24, dtype=np.int64)[:, None] * n + pts[None, :]).reshape(-1))
         return np.concatenate(parts) if parts else np.zeros(0, dtype=np.int64)
 
-    def packed_plan(self, device):
-        """Per level and peer, the device index lists of the packed exchange:
-        {level: ([(peer, send index)], [(peer, recv index)])}, messages in
-        global block order (both sides build them from the same global plan)."""
+    def packed_plan(self, device, phase: str = "fill"):
+        """Per level and peer, the device index lists of a phase's packed
+        exchange: {level: ([(peer, send index)], [(peer, recv index)])},
+        messages in global block order (both sides build them from the same
+        global plan)."""
         import torch
-        key = str(device)
+        key = (str(device), phase)
         if key in self._packed:
             return self._packed[key]
+        levels, send, recv, reads = self._phase(phase)
         plan = {}
-        for lvl in self.levels:
+        for lvl in levels:
             sends, recvs = [], []
             for q in range(self.world):
-                sp = [(q2, j) for q2, j in self.send.get(lvl, []) if q2 == q]
+                sp = [(q2, j) for q2, j in send.get(lvl, []) if q2 == q]
                 if sp:
-                    idx = self._pack_index(sp, lambda j, q=q: self._reads[q][(lvl, j)])
+                    idx = self._pack_index(sp, lambda j, q=q: reads[q][(lvl, j)])
                     sends.append((q, torch.from_numpy(idx).to(device)))
-                rp = [(p, j) for p, j in self.recv.get(lvl, []) if p == q]
+                rp = [(p, j) for p, j in recv.get(lvl, []) if p == q]
                 if rp:
-                    idx = self._pack_index(rp, lambda j: self._reads[self.rank][(lvl, j)])
+                    idx = self._pack_index(rp, lambda j: reads[self.rank][(lvl, j)])
                     recvs.append((q, torch.from_numpy(idx).to(device)))
             plan[lvl] = (sends, recvs)
         self._packed[key] = plan
         return plan
 
-    def exchange_bytes(self, packed: bool = True) -> int:
-        """Bytes this rank sends per fill (all levels), packed or whole blocks."""
+    def exchange_bytes(self, packed: bool = True, phase: str = "fill") -> int:
+        """Bytes this rank sends per pass of a phase (all levels), packed or
+        whole blocks."""
+        levels, send, _, reads = self._phase(phase)
         total = 0
-        for lvl in self.levels:
-            for q, j in self.send.get(lvl, []):
-                total += 8 * 24 * (len(self._reads[q][(lvl, j)]) if packed else self.pool.blocks[self.g2l[j]].points)
+        for lvl in levels:
+            for q, j in send.get(lvl, []):
+                total += 8 * 24 * (len(reads[q][(lvl, j)]) if packed else self.pool.blocks[self.g2l[j]].points)
         return total
 
-    def exchange_packed(self, pool_tensor, level: int, group=None) -> None:
-        """:meth:`exchange` moving only the points the receivers' fill boxes
-        read: one gathered buffer per peer and level each way, scattered into
-        the mirrors on arrival. Mirror points outside the read boxes are not
-        kept up to date (no fill box reads them)."""
+    def exchange_packed(self, pool_tensor, level: int, group=None, phase: str = "fill") -> None:
+        """:meth:`exchange` moving only the points the receivers' boxes read:
+        one gathered buffer per peer and level each way, scattered into the
+        mirrors on arrival. Mirror points outside the read boxes are not kept
+        up to date (no box reads them)."""
         import torch
         import torch.distributed as dist
         if self.world == 1:
             return
-        sends, recvs = self.packed_plan(pool_tensor.device)[level]
+        sends, recvs = self.packed_plan(pool_tensor.device, phase)[level]
         flat = pool_tensor.view(-1)
         ops, bufs = [], []
         for q, idx in sends:
@@ -236,16 +273,17 @@ class RankLayout:
         o = int(self.pool.offsets[i])
         return pool_tensor[o:o + 24 * self.pool.blocks[i].points]
 
-    def exchange(self, pool_tensor, level: int, group=None) -> None:
-        """Move the blocks the ``level`` fill reads across ranks: send this
-        rank's blocks that others mirror, receive its own mirrors."""
+    def exchange(self, pool_tensor, level: int, group=None, phase: str = "fill") -> None:
+        """Move the blocks a phase's ``level`` boxes read across ranks: send
+        this rank's blocks that others mirror, receive its own mirrors."""
         import torch.distributed as dist
         if self.world == 1:
             return
+        _, send, recv, _ = self._phase(phase)
         ops = []
-        for q, j in self.send.get(level, []):
+        for q, j in send.get(level, []):
             ops.append(dist.P2POp(dist.isend, self.block_view(pool_tensor, j), q, group=group))
-        for p, j in self.recv.get(level, []):
+        for p, j in recv.get(level, []):
             ops.append(dist.P2POp(dist.irecv, self.block_view(pool_tensor, j), p, group=group))
         if ops:
             for req in dist.batch_isend_irecv(ops):
@@ -262,23 +300,34 @@ class DistributedBatchedEvolution:
     between the launches). ``world == 1`` is the single-GPU exchange path."""
 
     def __init__(self, blocks: Sequence, punctures=None, world: int = 1, rank: int = 0, ko_sigma: float = 0.1,
-                 ko_order: int = 6, variant: int = 0, device="cuda", group=None, packed: bool = True):
-        from .amr import BatchedEvolution
-        self.layout = RankLayout(blocks, world, rank)
+                 ko_order: int = 6, variant: int = 0, device="cuda", group=None, packed: bool = True,
+                 restrict: bool = False):
+        from .amr import BatchedEvolution, BlockPool
+        from .ghosts import GhostPlan
+        self.layout = RankLayout(blocks, world, rank, plan=GhostPlan(BlockPool(blocks), restrict=restrict))
         self.group = group
         self.packed = bool(packed)
         self.evo = BatchedEvolution(self.layout.pool, ko_sigma=ko_sigma, ko_order=ko_order, variant=variant,
                                     device=device, ghosts="exchange", plan=self.layout,
                                     active=self.layout.owned)
 
-    def fill(self, Y) -> None:
+    def _run(self, phase: str, levels, Y) -> None:
         stream = self.evo._stream()
-        for lvl in self.layout.levels:
+        for lvl in levels:
             if self.packed:
-                self.layout.exchange_packed(Y, lvl, self.group)
+                self.layout.exchange_packed(Y, lvl, self.group, phase=phase)
             else:
-                self.layout.exchange(Y, lvl, self.group)
-            self.evo.dplan.run_level("fill", lvl, Y, stream)
+                self.layout.exchange(Y, lvl, self.group, phase=phase)
+            self.evo.dplan.run_level(phase, lvl, Y, stream)
+
+    def fill(self, Y) -> None:
+        """Ghost fill of Y, coarse level first, remote sources received per level."""
+        self._run("fill", self.layout.levels, Y)
+
+    def restrict(self, U) -> None:
+        """Injection of fine interiors into the coarser levels, finest first,
+        remote fine points received per level (``restrict=True``)."""
+        self._run("restrict", self.layout.restrict_levels, U)
 
     def step_inplace(self, U, S) -> None:
         b = self.evo.buffers(U)
@@ -286,6 +335,8 @@ class DistributedBatchedEvolution:
                                             (b["Ya"], U)]):
             self.fill(y)
             self.evo.stage(stage, U, y, b["ACC"], ynext, S)
+        if self.layout.restrict_levels:
+            self.restrict(U)
 
     def evolve(self, U, dt: float, nsteps: int, t0: float = 0.0):
         U = U.clone()

@@ -39,6 +39,9 @@ def _run_level(pool, lists, level, state):
             if op.kind == G.COPY:
                 s = d + sh
                 val = src[:, s[:, 0], s[:, 1], s[:, 2]]
+            elif op.kind == G.RESTRICT:
+                s = 2 * d + sh
+                val = src[:, s[:, 0], s[:, 1], s[:, 2]]
             else:
                 g = d + sh
                 val = A.refine(src)[:, g[:, 0], g[:, 1], g[:, 2]]
@@ -148,3 +151,58 @@ def test_packed_exchange_moves_only_the_read_points(world):
                     for y in (y0, y1 - 1):
                         for z in (z0, z1 - 1):
                             assert (x * sy + y) * sz + z in pts
+
+
+def _restrict_worker(rank, world, port, seed, out):
+    """Restriction across ranks: each rank injects (packed exchange of the
+    remote fine points, then its own restriction boxes) and its coarse
+    blocks equal the single-process injection."""
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from bssn3d_b200 import amr, ghosts
+        from bssn3d_b200.parallel import RankLayout
+        blocks = _blocks()
+        gpool = amr.BlockPool(blocks)
+        gplan = ghosts.GhostPlan(gpool, restrict=True)
+        state = np.random.default_rng(seed).standard_normal(gpool.size)
+        want = state.copy()
+        for lvl, _ in gplan.restrict_lists:          # the single process, finest first
+            _run_level(gpool, gplan.restrict_lists, lvl, want)
+        lay = RankLayout(blocks, world, rank, plan=gplan)
+        local = torch.zeros(lay.pool.size, dtype=torch.float64)
+        for i in lay.owned:
+            g = lay.index[i]
+            o = int(gpool.offsets[g])
+            lay.block_view(local, g).copy_(torch.from_numpy(state[o:o + 24 * blocks[g].points]))
+        arr = local.numpy()
+        for lvl in lay.restrict_levels:
+            lay.exchange_packed(local, lvl, phase="restrict")
+            _run_level(lay.pool, lay.restrict_lists, lvl, arr)
+        ok = True
+        for i in lay.owned:
+            g = lay.index[i]
+            o = int(gpool.offsets[g])
+            ok &= np.array_equal(lay.block_view(local, g).numpy(), want[o:o + 24 * blocks[g].points])
+        out[rank] = (int(ok), lay.exchange_bytes(True, "restrict"), lay.exchange_bytes(False, "restrict"))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_restrict_like_one_process(world):
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = ctx.Manager().dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_restrict_worker, args=(r, world, port, 5, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+        assert p.exitcode == 0
+    res = dict(out)
+    assert all(res[r][0] == 1 for r in range(world))
+    sent = sum(res[r][1] for r in range(world))
+    assert 0 < sent < sum(res[r][2] for r in range(world))   # the split cuts the injection, packed < whole

@@ -233,3 +233,8 @@ def test_distributed_evolution_one_rank_equals_batched_exchange():
     b = dist_evo.evolve(U, dt, 2)
     assert torch.equal(a, b)
     assert dist_evo.constraint_norms(b) == ref.constraint_norms(a)
+    # with restriction after every step
+    ref_r = amr.BatchedEvolution(pool, ko_sigma=0.1, ko_order=6, ghosts="exchange", restrict=True)
+    dist_r = DistributedBatchedEvolution(pool.blocks, world=1, rank=0, ko_sigma=0.1, ko_order=6, restrict=True)
+    assert ref_r.plan.restrict_lists and dist_r.layout.restrict_levels
+    assert torch.equal(ref_r.evolve(U, dt, 2), dist_r.evolve(U, dt, 2))
