@@ -129,7 +129,7 @@ def test_rhs_gauge_wave_golden():
     assert err.max() <= 1e-8
 
 
-@pytest.mark.parametrize("shape", [(20, 20, 20), (13, 27, 35), (4, 5, 40)])
+@pytest.mark.parametrize("shape", [(20, 20, 20), (13, 27, 35), (4, 5, 40), (40, 44, 50)])
 def test_rhs_random_state_vs_oracle(shape):
     F = _random_state(shape, sum(shape))
     S = _S(0.1, 0.11, 0.09, t=0.7)
