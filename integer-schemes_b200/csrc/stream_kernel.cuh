@@ -218,7 +218,7 @@ struct TileGeom {
   // (rows back to back) or exactly 16; the extra columns are never read.
   static constexpr int TROW = TZ + 6 <= 16 ? 16 : TP;
   static_assert(TROW <= TP, "T rows fit the pitch");
-  static constexpr int T1Y = TY + 6, T1N = TX * T1Y * TROW;  // d/dx over y and z halos
+  static constexpr int T1Y = TY + 6;                          // d/dx over the y halo (and the z halo of the central rows)
   static constexpr int T2N = TX * TY * TROW;                 // d/dy over the z halo
   static constexpr int T1VOL = TX * T1Y * TP, T2VOL = TX * TY * TP;
   static constexpr size_t SMEM = (2 * (size_t)VOL + T1VOL + T2VOL) * sizeof(double);
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
   constexpr int ZS = TMA ? Geo::ZS_TMA : 0;  // z shift of the staged rows
   // padded T rows only where their extra columns stay inside a staged row
   constexpr int TROW = Geo::TROW - 4 + R + ZS <= Geo::HZP - 1 ? Geo::TROW : TZ + 6;
-  constexpr int T1N = TX * Geo::T1Y * TROW, T2N = TX * TY * TROW;
+  constexpr int T2N = TX * TY * TROW;
   const int c = (lx + R) * Geo::SX + (ly + R) * Geo::SY + (lz + R + ZS);
   constexpr int st[3] = {Geo::SX, Geo::SY, 1};
   unsigned tphase = 0;    // bit b: parity of the next completion of tbar[b]
@@ -562,14 +562,24 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         }
       }
       if (has_d2(f)) {
-        // T1 = unscaled d/dx sums over x in [0,TX), y in [-3, TY+3), z in [-3, TZ+3)
-        for (int e = tid; e < T1N; e += NTHREADS) {
-          const int zz = e % TROW;
-          const int yy = (e / TROW) % Geo::T1Y;
-          const int xx = e / (TROW * Geo::T1Y);
+        // T1 = unscaled d/dx sums over x in [0,TX) on the L-shaped region the
+        // mixed taps read: y in [-3, TY+3) for z in [0, TZ) (for d2/dxdy), and
+        // y in [0, TY) for z in [-3, 0) and [TZ, TZ+3) (for d2/dxdz); T1 rows
+        // and columns are offset by 3 (row yy holds y = yy - 3).
+        for (int e = tid; e < TX * Geo::T1Y * TZ; e += NTHREADS) {
+          const int zz = e % TZ + 3;
+          const int yy = (e / TZ) % Geo::T1Y;
+          const int xx = e / (TZ * Geo::T1Y);
           const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R + ZS);
-          const double s = c1_at(cur + cc, Geo::SX);
-          T1[(xx * Geo::T1Y + yy) * HZP + zz] = s;
+          T1[(xx * Geo::T1Y + yy) * HZP + zz] = c1_at(cur + cc, Geo::SX);
+        }
+        for (int e = tid; e < TX * TY * 6; e += NTHREADS) {
+          const int k = e % 6;
+          const int zz = k < 3 ? k : TZ + k;
+          const int yy = (e / 6) % TY + 3;
+          const int xx = e / (6 * TY);
+          const int cc = (xx + R) * Geo::SX + (yy - 3 + R) * Geo::SY + (zz - 3 + R + ZS);
+          T1[(xx * Geo::T1Y + yy) * HZP + zz] = c1_at(cur + cc, Geo::SX);
         }
         // T2 = unscaled d/dy sums over x in [0,TX), y in [0,TY), z in [-3, TZ+3)
         for (int e = tid; e < T2N; e += NTHREADS) {
