@@ -10,9 +10,12 @@ interior points x 4 RHS evaluations per step / time (the reference's unit,
 3D/src/bssn3d/profile_regime.py:230). Inputs stay in HBM between steps and
 are larger than L2 (126 MB).
 
-For N > 1 (under torchrun) every rank evolves its own replica (the path has
-no exchange step at one block per GPU): weak scaling, value = total work of
-all ranks / max-over-ranks time.
+For N > 1 (under torchrun) every rank evolves its own replica by default:
+weak scaling, value = total work of all ranks / max-over-ranks time. With
+``--split slab`` the one block is cut into N x-slabs instead
+(``bssn3d_b200.slabs``: per stage, each rank's fused stage launch on its
+slab, then its halo planes from the neighbours over NCCL): strong scaling,
+value = the block's work / max-over-ranks time.
 
 ``--impl reference`` times the reference's own CPU algebra
 (oracle/_ref/libdendro_ref.so, compiled from the reference's vendored
@@ -64,6 +67,9 @@ def parse():
                          "INT8 tensor-core derivatives on the 192^3 block, k = 5..8")
     ap.add_argument("--integrator", default="rk4", choices=["rk4", "rk4_2_1", "rk4_2_2"],
                     help="uniform workload: RK4 or a 2-step/3-stage MSRK integrator")
+    ap.add_argument("--split", default="replicas", choices=["replicas", "slab"],
+                    help="bl128 at N > 1: N independent replicas (weak scaling, the default) or the one "
+                         "block cut into N x-slabs with a halo exchange per stage (strong scaling)")
     ap.add_argument("--ghosts", default="exchange", choices=["exchange", "evolve"],
                     help="block lists: refill ghosts from other blocks each stage, or evolve them")
     ap.add_argument("--track", type=int, default=0,
@@ -864,6 +870,136 @@ def bench_ozaki(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_slab(args):
+    """The 128^3 block split into x-slabs, one per rank (strong scaling)."""
+    import torch
+    world, rank, local = dist_env()
+    group = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    from bssn3d_b200 import initial_data as ID
+    from bssn3d_b200.slabs import SlabEvolution
+
+    grid, U_host, dt = ID.workload(1, n=args.n)
+    interior = grid.interior_points
+    evo = SlabEvolution(grid, world=world, rank=rank, ko_sigma=0.1, ko_order=6, group=group)
+    lay = evo.layout
+    U = evo.local(torch.from_numpy(U_host)).to(dev)
+    S = evo.scalars(0.0, dt, dev)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(ms):
+        if world > 1:
+            import torch.distributed as dist
+            t = torch.tensor([ms], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    for _ in range(args.warmup):
+        evo.step_inplace(U, S)
+        evo.advance_time(S)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    stream = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        evo.step_inplace(U, S)
+        evo.advance_time(S)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    finite = bool(torch.isfinite(evo.owned(U)).all().item())
+
+    # end to end: every step copies the rank's slab in from pinned host memory
+    # and its owned planes out
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(U_host[:, lay.local_slice()].copy()).pin_memory()
+        host_out = torch.empty_like(host_in[:, lay.owned_slice()]).pin_memory()
+        Ue, Se = torch.empty_like(U), evo.scalars(0.0, dt, dev)
+
+        def e2e_step():
+            Ue.copy_(host_in, non_blocking=True)
+            Se.copy_(S)
+            evo.step_inplace(Ue, Se)
+            host_out.copy_(evo.owned(Ue), non_blocking=True)
+        for _ in range(args.warmup):
+            e2e_step()
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        f1.record(stream)
+        barrier()
+        ems = max_over_ranks(f0.elapsed_time(f1))
+        nb = torch.tensor([host_in.numel() * 8, host_out.numel() * 8], dtype=torch.float64, device=dev)
+        if world > 1:
+            import torch.distributed as dist
+            dist.all_reduce(nb)
+        e2e = {"value": interior * 4 * args.steps / (ems * 1e-3) / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(nb[0].item()), "d2h_bytes_per_step": int(nb[1].item()),
+               "ms_per_step": ems / args.steps,
+               "path": "bssn3d_b200.slabs.SlabEvolution: per step and rank, its slab in from pinned "
+                       "host memory, one RK4 step with the halo exchanges, its owned planes out"}
+
+    # per-launch stage time on this rank's slab (the owned interior points it delivers)
+    b = evo.buffers(U)
+    durs = []
+    for _ in range(3):
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        evo.stage_fn(1, U, b["Ya"], b["ACC"], b["Yb"], S)
+        a1.record(stream)
+        a1.synchronize()
+        durs.append(a0.elapsed_time(a1))
+    stage_ms = statistics.median(durs)
+    ng = grid.ng
+    owned_interior = max(min(lay.b, lay.Sx - ng) - max(lay.a, ng), 0) * grid.Ny * grid.Nz
+    peaks, peak_kind = measured_peaks()
+    achieved = owned_interior * STAGE_BYTES / (stage_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                "frac": achieved / peaks.get("hbm_gbs"), "traffic": None,
+                "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel": "bssn::stream_kernel<3, MODE_STAGE, Shape<4,4,16>> on rank 0's slab",
+                "bytes_per_point_update": STAGE_BYTES, "point_updates_per_launch": owned_interior,
+                "points_evaluated_per_launch": int(U[0].numel()), "launch_ms": stage_ms}
+    value = interior * 4 * args.steps / (ms * 1e-3) / 1e6
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"Brill-Lindquist q=1/10, {args.n}^3 interior +3 ghosts on [-8,8]^3, "
+                               f"RK4 step, KO sigma 0.1 order 6, split into {world} x-slabs",
+                   "array": list(grid.shape), "slabs": lay.ranges, "halo_planes": lay.halo,
+                   "exchange_bytes_per_stage_rank0": lay.exchange_bytes(grid.shape[1], grid.shape[2]),
+                   "l2": "inputs larger than L2 (462 MB state)", "parallelism": f"slab x{world}"},
+        "clocks": clk, "gpu_launches": 5 * args.steps, "finite": finite, "roofline": roofline,
+        "e2e": e2e, "cpu_baseline": None,
+    }
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -872,6 +1008,8 @@ def main():
         bench_amr(args)
     elif args.workload == "ozaki192":
         bench_ozaki(args)
+    elif args.split == "slab":
+        bench_slab(args)
     else:
         bench_b200(args)
 
