@@ -76,6 +76,10 @@ def parse():
                     help="after timing, evolve this many more steps and record the constraint norms")
     ap.add_argument("--track-every", type=int, default=10)
     ap.add_argument("--blocks", type=int, default=0, help="amr3/amr4: block count instead of 600/2000 (small cases)")
+    ap.add_argument("--fill-split", action="store_true",
+                    help="amr3/amr4 with ghost exchange: also time each level's fill with its op list whole, "
+                         "its copy boxes alone and its prolongation boxes alone (NVTX ranges 'fill L<level> "
+                         "<part>' around each list's launches)")
     ap.add_argument("--ozaki-k", default="0",
                     help="ozaki192: one digit count instead of k = 5..8; amr3/amr4: evolve through the "
                          "Ozaki INT8 derivative path with this many digit planes (0 = float64 stencils, "
@@ -90,6 +94,57 @@ def parse():
     ap.add_argument("--no-m4", action="store_true",
                     help="bl128: skip the reference's M4 CUDA RHS measured beside the fused one")
     return ap.parse_args()
+
+
+def fill_split(evo, pool, Y, stream, dev, reps=10):
+    """Per level: the fill's op list timed whole, its copy boxes alone and its
+    prolongation boxes alone (each list uploaded through bssn_b200_fill_plan,
+    one warm-up launch, then ``reps`` launches between CUDA events, each list
+    inside the NVTX range 'fill L<level> <part>')."""
+    import ctypes
+    import torch
+    from bssn3d_b200 import _lib
+    from bssn3d_b200.ghosts import PROLONG, FillOp, W_MID
+    lib = _lib.load()
+    wmid = (ctypes.c_double * 6)(*W_MID)
+    sp = stream.cuda_stream
+
+    def upload(ops):
+        arr = (FillOp * len(ops))(*ops)
+        total = lib.bssn_b200_fill_plan(ctypes.addressof(arr), len(ops), int(pool.size))
+        if total < 0:
+            _lib.check(_lib.EINVAL)
+        raw = bytes(memoryview(arr).cast("B"))
+        return torch.frombuffer(bytearray(raw), dtype=torch.uint8).to(dev), len(ops), int(total)
+
+    def timed(ops, name):
+        dv, nops, npts = upload(ops)
+
+        def run():
+            _lib.check(lib.bssn_b200_fill(sp, Y.data_ptr(), dv.data_ptr(), nops, npts,
+                                          ctypes.cast(wmid, ctypes.c_void_p)))
+        torch.cuda.nvtx.range_push(name)
+        run()
+        torch.cuda.synchronize(dev)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            run()
+        b.record(stream)
+        b.synchronize()
+        torch.cuda.nvtx.range_pop()
+        return round(a.elapsed_time(b) / reps, 4), npts
+
+    out = []
+    for lvl, ops in evo.plan.fill_lists:
+        row = {"level": lvl, "ops": len(ops)}
+        row["whole_ms"], row["points"] = timed(list(ops), f"fill L{lvl} whole")
+        for part, keep in (("copy", lambda o: o.kind != PROLONG), ("prolong", lambda o: o.kind == PROLONG)):
+            sel = [o for o in ops if keep(o)]
+            if sel:
+                row[f"{part}_ms"], row[f"{part}_points"] = timed(sel, f"fill L{lvl} {part}")
+        out.append(row)
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -717,6 +772,10 @@ def bench_amr(args):
     if oz_k:
         breakdown["derivative_bundle_ms"] = ev_ms(lambda: evo.derivatives(Y_t, S_g))
     del Y_t
+    if args.fill_split and evo.plan is not None:
+        Y_s = U_g.clone()
+        breakdown["fill_split"] = fill_split(evo, pool, Y_s, stream, dev)
+        del Y_s
     fills = len(evo.dplan.fill) if evo.dplan is not None else 0
     ghost_counts = evo.plan.counts if evo.plan is not None else None
     variant = evo.variant
