@@ -464,6 +464,38 @@ def bench_b200(args):
                        "bssn_b200_rk4_stage, captured), result out; copies overlapped with the "
                        "neighbouring steps' compute"}
         del pipe
+        # the host link alone, the ceiling of the end-to-end rate: one state in
+        # and one state out at the same time, on two streams
+        s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+        d_in = torch.empty(U_host.shape, dtype=torch.float64, device=dev)
+        d_out = U_g.clone()
+
+        def link_once():
+            s_in.wait_stream(stream)
+            s_out.wait_stream(stream)
+            with torch.cuda.stream(s_in):
+                d_in.copy_(host_in, non_blocking=True)
+            with torch.cuda.stream(s_out):
+                host_out.copy_(d_out, non_blocking=True)
+            stream.wait_stream(s_in)
+            stream.wait_stream(s_out)
+        link_once()
+        torch.cuda.synchronize(dev)
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 5
+        l0.record(stream)
+        for _ in range(reps):
+            link_once()
+        l1.record(stream)
+        l1.synchronize()
+        link_ms = l0.elapsed_time(l1) / reps
+        dev_ms = ms / args.steps
+        e2e["link"] = {"ms_per_state_each_way": link_ms, "gbs_each_way": nbytes / (link_ms * 1e-3) / 1e9,
+                       "bound_value": interior * 4 * world / (max(link_ms, dev_ms) * 1e-3) / 1e6,
+                       "what": "one state copied in (pinned host to device) and one out at the same time on "
+                               "two streams; bound_value = the rate at max(link time, device step time)"}
+        e2e["frac_of_bound"] = e2e["value"] / e2e["link"]["bound_value"]
+        del d_in, d_out
 
     # the Ozaki INT8 half of the metric and the reference's M4 CUDA kernel, on
     # the same state (outside the timed region)
