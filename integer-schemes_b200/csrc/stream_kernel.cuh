@@ -504,6 +504,7 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
       stage_tile<R, T, ZS>(bufp(0), Fbase + (long long)stream_field(0) * n, x0, y0, z0, Sx, Sy, Sz, tid);
       cp_async_commit();
     }
+    const bool first_halo_old = prefetched;  // committed before this tile's point staging
     prefetched = false;
     Unroll<0, NFIELD>::run([&](auto ic) {
       constexpr int idx = decltype(ic)::value;
@@ -526,7 +527,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
         __syncthreads();
         if (idx + 1 < NFIELD) tma_issue(stream_field(idx + 1), (idx + 1) % NB);
       } else {
-        cp_async_wait<0>();
+        // field 0: a halo staged during the previous tile is older than the
+        // u_n / accumulator point staging, which may still be in flight
+        if (Geo::PTS && idx == 0 && first_halo_old) cp_async_wait<1>();
+        else cp_async_wait<0>();
         __syncthreads();
         if (idx + 1 < NFIELD) {
           stage_tile<R, T, ZS>(bufp((idx + 1) % NB), Fbase + (long long)stream_field(idx + 1) * n, x0, y0, z0,
