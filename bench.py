@@ -49,8 +49,8 @@ STAGE_BYTES = 960           # read Y, U, ACC; write ACC, Y_next (5 x 24 x 8 B)
 # DRAM bytes per evaluated point of one stage launch, dram__bytes_read.sum +
 # dram__bytes_write.sum from an ncu capture of the stage-1 kernel on the 102^3
 # case, scaled to a launch by its points (the capture is named here)
-TRAFFIC_BYTES_PER_POINT = 965
-TRAFFIC_SOURCE = "ncu capture, profiles/stream_kernel_stage_102.md (965 B per evaluated point)"
+TRAFFIC_BYTES_PER_POINT = 963
+TRAFFIC_SOURCE = "ncu capture, profiles/stream_kernel_stage_102.md (963 B per evaluated point)"
 LAST_STAGE_BYTES = 768      # read Y, U, ACC; write U_new
 
 
