@@ -431,8 +431,10 @@ __global__ void __launch_bounds__(NTHREADS, 1) stream_kernel(const Args args, co
                            clampll(gz, Sz - 1 - core);
     const double* __restrict__ Fbase = args.F + base;
     // Stage this point's 24 values (and, for the RK update, u_n and the
-    // accumulator) in shared memory with one batch of cp.async: each thread
-    // copies and later reads only its own slots, so no barrier is needed.
+    // accumulator) in shared memory with cp.async: each thread copies and
+    // later reads only its own slots, so no barrier is needed. Two commit
+    // groups: the stage input, waited for here, then u_n and the accumulator,
+    // read only by the epilogue and waited for at field 1 at the latest.
     if (Geo::PTS) {
 #pragma unroll
       for (int k = 0; k < NFIELD; ++k) cp_async8(pY + k * NTHREADS + tid, args.F + gidx + (long long)k * n);
